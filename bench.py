@@ -1,0 +1,390 @@
+"""Throughput of the B200 direction-optimizing BFS (one JSON line on stdout).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--graph rmat24|uniform24|grid4096|rmatS]
+                    [--roots 64] [--impl nwg|reference]
+
+Workload (default): RMAT scale 24, edge factor 16, A/B/C/D = .57/.19/.19/.05,
+ids permuted, symmetrized, deduplicated, self-loops removed (uint32 columns,
+uint64 offsets), generated on the device from a fixed seed; 64 roots drawn
+uniformly among vertices with out-degree > 0 (seed 27491095).  One "step" is
+the 64 single-source traversals.
+
+Metric: GTEPS = (E_r / 2) / t per root, E_r = sum of out-degrees of the
+vertices the root reaches (directed CSR entries, Graph500 convention),
+harmonic mean over the roots; t = device time of the whole traversal
+(initialisation of parents and bitmaps included, like the reference's bfs()
+call) from CUDA events on the launching stream.  The L2 is flushed (256 MB
+write) before every traversal, outside the events.
+
+e2e: the same metric through the C ABI with host buffers: each step
+registers the graph from pinned host CSR arrays (the upload), runs the 64
+nwg_bfs calls each copying the parents back to pinned host memory, and
+releases the graph; per-root time = call time + 1/64 of the upload.
+
+roofline: algorithmic bytes of a traversal B_r = 4 E_r + 8 n_r + 4 N
+(every adjacency entry of the component, one offset per reached vertex,
+the parent array) over its device time, against the measured HBM copy
+bandwidth.
+
+cpu_baseline / --impl reference: the reference's own nw::graph::bfs
+(include/nwgraph/algorithms/bfs.hpp, compiled unmodified against the
+project's TBB-compatible thread pool, oracle/_ref) on this host's cores,
+timed like bench/common.hpp's time_op, on a bounded sample of the roots.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+ROOT_SEED = 27491095
+GRAPH_SEED = 1
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--graph", default="rmat24")
+    ap.add_argument("--roots", type=int, default=64)
+    ap.add_argument("--impl", default="nwg", choices=["nwg", "reference"])
+    ap.add_argument("--cpu-sample-roots", type=int, default=4)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile-one", action="store_true",
+                    help="after warm-up, run one traversal inside an NVTX range 'nwg_profile' and exit (for ncu)")
+    return ap.parse_args()
+
+
+def graph_spec(name: str):
+    if name == "rmat24":
+        return {"kind": "rmat", "scale": 24, "edge_factor": 16}
+    if name.startswith("rmat"):
+        return {"kind": "rmat", "scale": int(name[4:]), "edge_factor": 16}
+    if name == "uniform24":
+        return {"kind": "uniform", "n": 1 << 24, "avg_degree": 32}
+    if name.startswith("uniform"):
+        return {"kind": "uniform", "n": 1 << int(name[7:]), "avg_degree": 32}
+    if name == "grid4096":
+        return {"kind": "grid", "width": 4096, "height": 4096, "shortcut_pct": 1}
+    raise SystemExit(f"unknown graph {name}")
+
+
+def make_graph(nwg, spec):
+    if spec["kind"] == "rmat":
+        return nwg.Graph.rmat(spec["scale"], spec["edge_factor"], seed=GRAPH_SEED)
+    if spec["kind"] == "uniform":
+        return nwg.Graph.uniform(spec["n"], spec["avg_degree"], seed=GRAPH_SEED)
+    return nwg.Graph.grid(spec["width"], spec["height"], spec["shortcut_pct"], seed=GRAPH_SEED)
+
+
+def workload_name(spec):
+    if spec["kind"] == "rmat":
+        return f"RMAT-{spec['scale']} ef{spec['edge_factor']} .57/.19/.19/.05 permuted symmetrized dedup"
+    if spec["kind"] == "uniform":
+        return f"uniform n={spec['n']} avg degree {spec['avg_degree']}"
+    return f"grid {spec['width']}x{spec['height']} 4-neighbour + {spec['shortcut_pct']}% shortcuts"
+
+
+def hmean(x):
+    x = np.asarray(x, dtype=np.float64)
+    return float(x.size / np.sum(1.0 / x))
+
+
+def peaks():
+    try:
+        with open(PEAKS_FILE) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.3)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = [r for r in self.rows if len(r) >= 9]
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference_arm(args, spec, world, rank):
+    """The reference's own CPU bfs on this host (rank 0 only)."""
+    if rank != 0:
+        return
+    import torch  # noqa: F401  (device for graph generation only)
+
+    import nwgr_b200 as nwg
+    from oracle.oracle import Reference
+
+    ref = Reference()
+    g = make_graph(nwg, spec)
+    off, cols = g.csr()
+    roots = g.roots(args.roots, seed=ROOT_SEED)
+    deg = off[1:] - off[:-1]
+    g.release()
+    rg = ref.graph(off, cols)
+    threads = ref.threads()
+    per_step = max(1, args.cpu_sample_roots)
+    times, edges, k = [], [], 0
+    for step in range(args.warmup + args.steps):
+        for _ in range(per_step):
+            r = int(roots[k % roots.size])
+            k += 1
+            parents, secs = rg.dobfs(r, 32, 15, 18)
+            if step >= args.warmup:
+                reached = parents != 0xFFFFFFFF
+                times.append(secs)
+                edges.append(float(deg[reached].sum()) / 2.0)
+    rg.close()
+    gteps = [e / t / 1e9 for e, t in zip(edges, times)]
+    v = hmean(gteps)
+    sample = (f"{per_step} roots per step ({len(times)} timed) of the {roots.size}-root workload, "
+              f"reference bfs.hpp on the project's TBB-compatible pool, {threads} threads")
+    line = {
+        "impl": "reference", "metric": f"BFS GTEPS (harmonic mean over roots) @ {args.graph}", "value": v,
+        "unit": "GTEPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * float(np.sum(times)) / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "uint32", "data": "synthetic (seeded generator)",
+        "config": {"workload": workload_name(spec), "roots": int(roots.size), "alpha": 15, "beta": 18},
+        "cpu_baseline": {"value": v, "unit": "GTEPS", "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": v, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(off, cols, roots, n_roots):
+    """Reference bfs.hpp on the host cores over a bounded sample of roots."""
+    from oracle.oracle import Reference
+
+    try:
+        ref = Reference()
+    except (FileNotFoundError, OSError) as e:
+        return {"value": None, "unit": "GTEPS", "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}
+    deg = off[1:] - off[:-1]
+    rg = ref.graph(off, cols)
+    rg.dobfs(int(roots[0]), 32, 15, 18, want_parents=False)  # warm the pool and pages
+    gteps = []
+    for r in roots[:n_roots]:
+        parents, secs = rg.dobfs(int(r), 32, 15, 18)
+        gteps.append(float(deg[parents != 0xFFFFFFFF].sum()) / 2.0 / secs / 1e9)
+    rg.close()
+    return {"value": hmean(gteps), "unit": "GTEPS", "cores": ref.threads(), "kind": "reference",
+            "sample": f"first {len(gteps)} of the {len(roots)} roots, reference bfs.hpp on the project's "
+                      f"TBB-compatible pool, wall clock around each call (time_op)"}
+
+
+def main():
+    args = parse()
+    spec = graph_spec(args.graph)
+    world, rank, local = dist_setup(args)
+    import torch
+
+    if args.impl == "reference":
+        if world > 1:
+            torch.cuda.set_device(local)
+        run_reference_arm(args, spec, world, rank)
+        return
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    import nwgr_b200 as nwg
+
+    g = make_graph(nwg, spec)
+    n, m = g.n, g.m
+    roots = g.roots(args.roots, seed=ROOT_SEED)
+    stream = torch.cuda.Stream()
+    ws = g.workspace()
+    parents = torch.empty(n, dtype=torch.int32, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    # per-root work (E_r, n_r) and launch counts from one untimed pass
+    e_r, n_r, launches = [], [], []
+    for r in roots:
+        with torch.cuda.stream(stream):
+            ws.bfs_async(int(r), parents, stream.cuda_stream)
+        stream.synchronize()
+        st = ws.stats()
+        if st.status != 0:
+            raise SystemExit(f"traversal from root {int(r)} reported status {st.status}")
+        e, v = g.component_edges(parents)
+        e_r.append(e)
+        n_r.append(v)
+        launches.append(2 * st.steps + 2)  # init + decide per iteration (+1 final) + one action per step
+    e_r = np.asarray(e_r, np.float64)
+    n_r = np.asarray(n_r, np.float64)
+
+    if args.profile_one:
+        with torch.cuda.stream(stream):
+            ws.bfs_async(int(roots[0]), parents, stream.cuda_stream)
+        stream.synchronize()
+        torch.cuda.nvtx.range_push("nwg_profile")
+        with torch.cuda.stream(stream):
+            ws.bfs_async(int(roots[0]), parents, stream.cuda_stream)
+        stream.synchronize()
+        torch.cuda.nvtx.range_pop()
+        print(json.dumps({"profile_one": True, "root": int(roots[0]), "n": n, "m": m}))
+        return
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in roots]
+
+    def one_step(record):
+        for i, r in enumerate(roots):
+            with torch.cuda.stream(stream):
+                flush.fill_(i & 0xFF)
+                ev[i][0].record(stream)
+                ws.bfs_async(int(r), parents, stream.cuda_stream)
+                ev[i][1].record(stream)
+        stream.synchronize()
+        if record is not None:
+            record.append([ev[i][0].elapsed_time(ev[i][1]) for i in range(len(roots))])
+
+    for _ in range(args.warmup):
+        one_step(None)
+    clocks = ClockSampler(local)
+    clocks.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rec = []
+    for _ in range(args.steps):
+        one_step(rec)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+
+    per_root_ms = np.mean(np.asarray(rec), axis=0)  # mean over steps, per root
+    if dist:
+        t = torch.tensor(per_root_ms, device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        per_root_ms = t.cpu().numpy()
+    gteps = (e_r / 2.0) / (per_root_ms * 1e-3) / 1e9
+    value = world * hmean(gteps)
+    hbm, hbm_kind = peaks()
+    b_r = 4.0 * e_r + 8.0 * n_r + 4.0 * n
+    achieved_gbs = float(np.mean(b_r / (per_root_ms * 1e-3)) / 1e9)
+    traffic = os.environ.get("NWG_TRAFFIC_BYTES")
+
+    # e2e through the C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        off, cols = g.csr()
+        off_p = torch.from_numpy(off.view(np.int64)).pin_memory()
+        col_p = torch.from_numpy(cols.view(np.int32)).pin_memory()
+        par_h = torch.empty(n, dtype=torch.int32).pin_memory()
+        h2d = off.nbytes + cols.nbytes
+        e2e_vals = []
+        for step in range(1 + args.steps):
+            t_up = time.perf_counter()
+            ge = nwg.Graph.from_csr(off_p.numpy().view(np.uint64), col_p.numpy().view(np.uint32))
+            up = time.perf_counter() - t_up
+            ts = []
+            for r in roots:
+                t1 = time.perf_counter()
+                nwg.bfs(ge, ge, int(r), parents_out=par_h.numpy().view(np.uint32))
+                ts.append(time.perf_counter() - t1 + up / len(roots))
+            ge.release()
+            if step > 0:
+                e2e_vals.append(hmean((e_r / 2.0) / np.asarray(ts) / 1e9))
+        e2e = {"value": float(np.mean(e2e_vals)) * world, "unit": "GTEPS", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(4 * n * len(roots)),
+               "note": "per step: upload CSR from pinned host memory, 64 nwg_bfs calls each returning parents "
+                       "to pinned host memory, release"}
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        off, cols = g.csr()
+        cpu = cpu_baseline(off, cols, roots, args.cpu_sample_roots)
+
+    if rank == 0:
+        line = {
+            "metric": f"BFS GTEPS (harmonic mean over {len(roots)} roots) @ {args.graph}, device time",
+            "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": float(np.sum(per_root_ms)), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "uint32", "data": "synthetic (seeded device generator)",
+            "config": {"workload": workload_name(spec), "n": n, "m_directed": m, "roots": len(roots),
+                       "alpha": 15, "beta": 18, "l2": "flushed (256 MB write) before every traversal",
+                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+            "gteps_min": float(np.min(gteps)), "gteps_max": float(np.max(gteps)),
+            "ms_per_root_median": float(np.median(per_root_ms)), "wall_s_timed": wall,
+            "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved_gbs / hbm, "peak_kind": hbm_kind,
+                         "kernel": "one traversal (level-loop CUDA graph: k_init, k_decide, k_td, k_bu, k_b2q)",
+                         "algorithmic_bytes_per_launch_mean": float(np.mean(b_r)),
+                         "traffic": float(traffic) if traffic else None},
+            "gpu_launches": int(np.sum(launches)) * args.steps,
+            "clocks": clk, "e2e": e2e, "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    ws.close()
+    g.release()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,150 @@
+/*
+ * nwg_bfs.h -- C ABI of the B200 direction-optimizing BFS library
+ * (libnwgr_b200.so).  Plain pointers and sizes only; every function returns
+ * an int status (0 = NWG_OK, negative = error, message via nwg_last_error).
+ * No exception crosses this boundary.
+ *
+ * Each entry point names the NWGraph interface it replaces (paths relative
+ * to the NWGraph source tree).  NWGraph is header-only C++; its BFS has no
+ * ABI of its own, so these functions are what a C++ wrapper (the drop-in
+ * header include/nwgraph/algorithms/bfs.hpp of this repository) or a foreign
+ * function interface binds to.
+ *
+ * Graphs are CSR: offsets (n+1 entries, uint64 or uint32) and uint32 column
+ * indices, rows in any order (the bottom-up step takes the first in-neighbour
+ * in row order, as the reference does).  The in-graph must be the transpose
+ * of the out-graph (the reference's contract for bfs(out, in, ...)); pass
+ * NULL in-pointers when the graph is symmetric and out == in.
+ */
+#ifndef NWG_BFS_H
+#define NWG_BFS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define NWG_OK 0
+#define NWG_EINVAL (-1)     /* bad argument: root >= n, alpha/beta <= 0, malformed CSR */
+#define NWG_ENOMEM (-2)     /* device or pinned allocation failed */
+#define NWG_ECUDA (-3)      /* CUDA runtime error */
+#define NWG_ETIMEDOUT (-4)  /* a bounded device loop or wait ran out */
+#define NWG_EOVERFLOW (-5)  /* a result does not fit its encoding (e.g. uint8 depth) */
+#define NWG_ESTATE (-6)     /* call out of order (e.g. stats before a traversal) */
+
+#define NWG_NULL_VERTEX 0xFFFFFFFFu /* null_vertex_v<uint32_t>(), util/util.hpp:125-132 */
+
+/* nwg_graph_register flags */
+#define NWG_REG_DEVICE 0x1u   /* arrays are device pointers, borrowed (not copied); caller keeps them alive */
+#define NWG_REG_VALIDATE 0x2u /* check monotone offsets and column ids < n before upload (host arrays) */
+
+typedef struct nwg_graph_s* nwg_graph;   /* a CSR pair resident in HBM */
+typedef struct nwg_bfs_ws_s* nwg_bfs_ws; /* per-traversal device state; one traversal in flight per workspace */
+
+#define NWG_TRACE_CAP 256
+
+/* Per-traversal statistics, read back once after the traversal. */
+typedef struct {
+  int32_t status;      /* device-side status of the traversal (0 = ok) */
+  uint32_t steps;      /* actions run by the level loop (top-down steps + bottom-up pulls + conversions) */
+  uint32_t levels;     /* BFS levels = maximum depth + 1 */
+  uint32_t td_steps;   /* top-down steps */
+  uint32_t bu_steps;   /* bottom-up pulls */
+  uint32_t b2q_steps;  /* bitmap-to-queue conversions */
+  uint64_t reached;    /* vertices with a parent, root included */
+  float device_ms;     /* device time of the traversal (CUDA events), 0 for the async API */
+  uint32_t trace_len;  /* records in the trace below (<= NWG_TRACE_CAP) */
+  /* one record per top-down step (dir 0) and bottom-up pull (dir 1), in order;
+   * frontier = queue size entering a top-down step, or the previous awake
+   * count entering a pull (bfs.hpp:205-209); found = vertices discovered */
+  uint8_t trace_dir[NWG_TRACE_CAP];
+  uint64_t trace_frontier[NWG_TRACE_CAP];
+  uint64_t trace_found[NWG_TRACE_CAP];
+} nwg_bfs_stats;
+
+/* Library version string. */
+const char* nwg_version(void);
+
+/* Copies the calling thread's last error message into buf (NUL-terminated).
+ * Returns the message length. */
+int nwg_last_error(char* buf, size_t len);
+
+/* Registers a CSR pair on the current CUDA device.  Replaces the CSR access
+ * that nw::graph::bfs performs on its arguments: out_graph.indices_ /
+ * std::get<0>(out_graph.to_be_indexed_) (containers/compressed.hpp:67-68,
+ * algorithms/bfs.hpp:168) and in_graph[u] (bfs.hpp:216).  Host arrays are
+ * uploaded once (the only bulk host-to-device copy); with NWG_REG_DEVICE
+ * they are borrowed in place.  in_off/in_col NULL = symmetric graph. */
+int nwg_graph_register(const uint64_t* out_off, const uint32_t* out_col, uint64_t n, const uint64_t* in_off,
+                       const uint32_t* in_col, uint32_t flags, nwg_graph* out);
+
+/* Same for NWGraph's default adjacency<0> layout, uint32 offsets
+ * (util/defaults.hpp:23-24); offsets are widened to uint64 on the device. */
+int nwg_graph_register_u32off(const uint32_t* out_off, const uint32_t* out_col, uint64_t n, const uint32_t* in_off,
+                              const uint32_t* in_col, uint32_t flags, nwg_graph* out);
+
+/* Frees the device copy (and every workspace created on it). */
+int nwg_graph_release(nwg_graph g);
+
+/* n, m (out-graph entries) and in_m of a registered graph; any may be NULL. */
+int nwg_graph_info(nwg_graph g, uint64_t* n, uint64_t* m, uint64_t* in_m);
+
+/* Direction-optimizing BFS from root; replaces nw::graph::bfs(out_graph,
+ * in_graph, root, num_bins, alpha, beta) (algorithms/bfs.hpp:160-311).
+ * num_bins has no GPU meaning (the device bins by degree) and is not taken.
+ * parents_host: host array of n entries (pageable or pinned) or NULL;
+ * parents_dev: device array of n entries or NULL; stats: NULL or filled.
+ * Unreached vertices get NWG_NULL_VERTEX, the root gets itself.
+ * Synchronous; thread-safe per graph (calls on one graph serialise). */
+int nwg_bfs(nwg_graph g, uint32_t root, int alpha, int beta, uint32_t* parents_host, uint32_t* parents_dev,
+            nwg_bfs_stats* stats);
+
+/* Workspaces for concurrent, stream-ordered traversals of one graph. */
+int nwg_ws_create(nwg_graph g, nwg_bfs_ws* out);
+int nwg_ws_destroy(nwg_bfs_ws ws);
+
+/* Stream-ordered variant of nwg_bfs: enqueues the whole traversal (one CUDA
+ * graph launch, no host synchronisation) on `stream` (a cudaStream_t, NULL =
+ * legacy default stream) writing parents to the device array parents_dev.
+ * At most one traversal per workspace may be in flight. */
+int nwg_bfs_async(nwg_bfs_ws ws, uint32_t root, int alpha, int beta, uint32_t* parents_dev, void* stream);
+
+/* Statistics of the workspace's last traversal; synchronises with it. */
+int nwg_ws_stats(nwg_bfs_ws ws, nwg_bfs_stats* stats);
+
+/* Top-down-only BFS (no in-graph needed); replaces the one-graph
+ * nw::graph::bfs(graph, root) (algorithms/bfs.hpp:110-140). */
+int nwg_bfs_topdown(nwg_graph g, uint32_t root, uint32_t* parents_host, uint32_t* parents_dev, nwg_bfs_stats* stats);
+
+/* Sum of out-degrees and count of the vertices reached in a device parents
+ * array (the TEPS numerator of a traversal); both outputs may be NULL. */
+int nwg_component_edges(nwg_graph g, const uint32_t* parents_dev, uint64_t* edges, uint64_t* vertices);
+
+/* Copies a registered graph's out-CSR (and in-CSR when not symmetric) to
+ * host arrays of the sizes nwg_graph_info reports; any pointer may be NULL. */
+int nwg_graph_copy_csr(nwg_graph g, uint64_t* out_off, uint32_t* out_col, uint64_t* in_off, uint32_t* in_col);
+
+/* Seeded synthetic graph generators on the device (no reference
+ * counterpart: NWGraph ships no RMAT/uniform/grid generator).  Each builds a
+ * symmetrized, self-loop-free, deduplicated CSR with sorted rows directly in
+ * HBM and registers it (symmetric: out == in).
+ * rmat: 2^scale vertices, edge_factor * 2^scale undirected draws with 32-bit
+ *       cumulative quadrant thresholds ta < tab < tabc, ids permuted.
+ * uniform: n vertices, n * avg_degree / 2 uniform random pairs.
+ * grid: width x height 4-neighbour grid plus shortcut_pct % random pairs. */
+int nwg_gen_rmat(uint32_t scale, uint32_t edge_factor, uint64_t seed, uint32_t ta, uint32_t tab, uint32_t tabc,
+                 nwg_graph* out);
+int nwg_gen_uniform(uint64_t n, uint32_t avg_degree, uint64_t seed, nwg_graph* out);
+int nwg_gen_grid(uint32_t width, uint32_t height, uint32_t shortcut_pct, uint64_t seed, nwg_graph* out);
+
+/* `count` roots uniform on [0, n) with out-degree > 0 (seeded). */
+int nwg_pick_roots(nwg_graph g, uint64_t seed, uint32_t count, uint32_t* roots_host);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NWG_BFS_H */

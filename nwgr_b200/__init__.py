@@ -1,0 +1,362 @@
+"""nwgr_b200 -- B200-native direction-optimizing BFS behind NWGraph's interface.
+
+Python host side of libnwgr_b200.so (C ABI: include/nwg_bfs.h).  The
+functions mirror NWGraph's BFS header, include/nwgraph/algorithms/bfs.hpp:
+
+    bfs(out_graph, in_graph, root, num_bins=32, alpha=15, beta=18) -> parents
+        nw::graph::bfs, bfs.hpp:160-311 (direction-optimizing)
+    bfs_serial(graph, root) -> parents
+        nw::graph::bfs(graph, root), bfs.hpp:110-140 (top-down only)
+    bfs_verifier(out_graph, in_graph, root, parents) -> bool
+        nw::graph::BFSVerifier, bfs.hpp:44-98 (host check)
+
+Graphs are registered once (uploaded to HBM) and reused by every call; the
+traversal runs entirely on the GPU.  There is no CPU fallback: importing the
+package raises if the CUDA library is missing, and every call raises
+NwgError on a non-zero status.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libnwgr_b200.so")
+
+NULL_VERTEX = 0xFFFFFFFF
+TRACE_CAP = 256
+
+NWG_OK, NWG_EINVAL, NWG_ENOMEM, NWG_ECUDA, NWG_ETIMEDOUT, NWG_EOVERFLOW, NWG_ESTATE = 0, -1, -2, -3, -4, -5, -6
+REG_DEVICE = 0x1
+REG_VALIDATE = 0x2
+
+# Every symbol include/nwg_bfs.h declares (checked by the CPU test suite).
+EXPORTED = (
+    "nwg_version", "nwg_last_error", "nwg_graph_register", "nwg_graph_register_u32off", "nwg_graph_release",
+    "nwg_graph_info", "nwg_bfs", "nwg_ws_create", "nwg_ws_destroy", "nwg_bfs_async", "nwg_ws_stats",
+    "nwg_bfs_topdown", "nwg_component_edges", "nwg_graph_copy_csr", "nwg_gen_rmat", "nwg_gen_uniform",
+    "nwg_gen_grid", "nwg_pick_roots",
+)
+
+
+class NwgError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"nwg error {code}: {msg}")
+        self.code = code
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("status", C.c_int32), ("steps", C.c_uint32), ("levels", C.c_uint32), ("td_steps", C.c_uint32),
+        ("bu_steps", C.c_uint32), ("b2q_steps", C.c_uint32), ("reached", C.c_uint64), ("device_ms", C.c_float),
+        ("trace_len", C.c_uint32), ("trace_dir", C.c_uint8 * TRACE_CAP),
+        ("trace_frontier", C.c_uint64 * TRACE_CAP), ("trace_found", C.c_uint64 * TRACE_CAP),
+    ]
+
+    def trace(self):
+        k = self.trace_len
+        return {
+            "dir": np.frombuffer(bytes(self.trace_dir), np.uint8)[:k].copy(),
+            "frontier": np.ctypeslib.as_array(self.trace_frontier)[:k].copy(),
+            "found": np.ctypeslib.as_array(self.trace_found)[:k].copy(),
+        }
+
+
+_vp = C.c_void_p
+_u32, _u64, _int = C.c_uint32, C.c_uint64, C.c_int
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is not built; run `python -m nwgr_b200.build` (nvcc, sm_100a)")
+    lib = C.CDLL(LIB_PATH)
+    sig = {
+        "nwg_version": (C.c_char_p, []),
+        "nwg_last_error": (_int, [C.c_char_p, C.c_size_t]),
+        "nwg_graph_register": (_int, [_vp, _vp, _u64, _vp, _vp, _u32, C.POINTER(_vp)]),
+        "nwg_graph_register_u32off": (_int, [_vp, _vp, _u64, _vp, _vp, _u32, C.POINTER(_vp)]),
+        "nwg_graph_release": (_int, [_vp]),
+        "nwg_graph_info": (_int, [_vp, C.POINTER(_u64), C.POINTER(_u64), C.POINTER(_u64)]),
+        "nwg_bfs": (_int, [_vp, _u32, _int, _int, _vp, _vp, C.POINTER(Stats)]),
+        "nwg_ws_create": (_int, [_vp, C.POINTER(_vp)]),
+        "nwg_ws_destroy": (_int, [_vp]),
+        "nwg_bfs_async": (_int, [_vp, _u32, _int, _int, _vp, _vp]),
+        "nwg_ws_stats": (_int, [_vp, C.POINTER(Stats)]),
+        "nwg_bfs_topdown": (_int, [_vp, _u32, _vp, _vp, C.POINTER(Stats)]),
+        "nwg_component_edges": (_int, [_vp, _vp, C.POINTER(_u64), C.POINTER(_u64)]),
+        "nwg_graph_copy_csr": (_int, [_vp, _vp, _vp, _vp, _vp]),
+        "nwg_gen_rmat": (_int, [_u32, _u32, _u64, _u32, _u32, _u32, C.POINTER(_vp)]),
+        "nwg_gen_uniform": (_int, [_u64, _u32, _u64, C.POINTER(_vp)]),
+        "nwg_gen_grid": (_int, [_u32, _u32, _u32, _u64, C.POINTER(_vp)]),
+        "nwg_pick_roots": (_int, [_vp, _u64, _u32, _vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(1024)
+    lib.nwg_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(rc: int) -> None:
+    if rc != NWG_OK:
+        raise NwgError(rc, last_error())
+
+
+def version() -> str:
+    return lib.nwg_version().decode()
+
+
+def _ptr(a) -> int | None:
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):  # torch tensor
+        return a.data_ptr()
+    return int(a)
+
+
+def rmat_thresholds(a: float = 0.57, b: float = 0.19, c: float = 0.19):
+    return int(a * 4294967296.0), int((a + b) * 4294967296.0), int((a + b + c) * 4294967296.0)
+
+
+class Graph:
+    """A CSR pair registered in HBM (nwg_graph).  `in_off`/`in_cols` None
+    means symmetric (the in-graph is the out-graph)."""
+
+    def __init__(self, handle: int, keep=None):
+        self.h = handle
+        self._keep = keep
+        n, m, im = _u64(), _u64(), _u64()
+        check(lib.nwg_graph_info(handle, C.byref(n), C.byref(m), C.byref(im)))
+        self.n, self.m, self.in_m = n.value, m.value, im.value
+
+    @classmethod
+    def from_csr(cls, off, cols, in_off=None, in_cols=None, validate=False, device=False):
+        """Registers host numpy CSR arrays (uploaded once) or, with
+        device=True, device arrays given as torch tensors / integer pointers
+        (borrowed).  uint32 offsets select the adjacency<0> layout."""
+        h = _vp()
+        flags = (REG_VALIDATE if validate else 0) | (REG_DEVICE if device else 0)
+        if device:
+            n = int(off.numel() - 1) if hasattr(off, "numel") else None
+            if n is None:
+                raise ValueError("device registration needs tensors")
+            fn = lib.nwg_graph_register if off.element_size() == 8 else lib.nwg_graph_register_u32off
+            check(fn(_ptr(off), _ptr(cols), n, _ptr(in_off), _ptr(in_cols), flags, C.byref(h)))
+            return cls(h.value, keep=(off, cols, in_off, in_cols))
+        off = np.ascontiguousarray(off)
+        cols = np.ascontiguousarray(cols, dtype=np.uint32)
+        if off.dtype == np.uint32:
+            fn = lib.nwg_graph_register_u32off
+            if in_off is not None:
+                in_off = np.ascontiguousarray(in_off, dtype=np.uint32)
+        else:
+            off = off.astype(np.uint64, copy=False)
+            fn = lib.nwg_graph_register
+            if in_off is not None:
+                in_off = np.ascontiguousarray(in_off, dtype=np.uint64)
+        if in_cols is not None:
+            in_cols = np.ascontiguousarray(in_cols, dtype=np.uint32)
+        check(fn(_ptr(off), _ptr(cols), off.size - 1, _ptr(in_off), _ptr(in_cols), flags, C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def rmat(cls, scale: int, edge_factor: int = 16, seed: int = 1, a=0.57, b=0.19, c=0.19):
+        h = _vp()
+        ta, tab, tabc = rmat_thresholds(a, b, c)
+        check(lib.nwg_gen_rmat(scale, edge_factor, seed, ta, tab, tabc, C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def uniform(cls, n: int, avg_degree: int = 32, seed: int = 1):
+        h = _vp()
+        check(lib.nwg_gen_uniform(n, avg_degree, seed, C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def grid(cls, width: int, height: int, shortcut_pct: int = 1, seed: int = 1):
+        h = _vp()
+        check(lib.nwg_gen_grid(width, height, shortcut_pct, seed, C.byref(h)))
+        return cls(h.value)
+
+    def csr(self):
+        """Host copy of the out-CSR (offsets uint64, columns uint32)."""
+        off = np.empty(self.n + 1, np.uint64)
+        cols = np.empty(self.m, np.uint32)
+        check(lib.nwg_graph_copy_csr(self.h, _ptr(off), _ptr(cols), None, None))
+        return off, cols
+
+    def roots(self, count: int = 64, seed: int = 27491095):
+        out = np.empty(count, np.uint32)
+        check(lib.nwg_pick_roots(self.h, seed, count, _ptr(out)))
+        return out
+
+    def component_edges(self, parents_dev):
+        e, v = _u64(), _u64()
+        check(lib.nwg_component_edges(self.h, _ptr(parents_dev), C.byref(e), C.byref(v)))
+        return e.value, v.value
+
+    def workspace(self):
+        return Workspace(self)
+
+    def release(self):
+        if self.h:
+            check(lib.nwg_graph_release(self.h))
+            self.h = None
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib.nwg_graph_release(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+class Workspace:
+    """Per-traversal device state for stream-ordered traversals (nwg_bfs_ws)."""
+
+    def __init__(self, g: Graph):
+        self.g = g
+        h = _vp()
+        check(lib.nwg_ws_create(g.h, C.byref(h)))
+        self.h = h.value
+
+    def bfs_async(self, root: int, parents_dev, stream=None, alpha=15, beta=18):
+        check(lib.nwg_bfs_async(self.h, int(root), alpha, beta, _ptr(parents_dev), _ptr(stream)))
+
+    def stats(self) -> Stats:
+        s = Stats()
+        check(lib.nwg_ws_stats(self.h, C.byref(s)))
+        return s
+
+    def close(self):
+        if self.h and self.g.h:
+            check(lib.nwg_ws_destroy(self.h))
+        self.h = None
+
+
+def bfs(out_graph: Graph, in_graph: Graph | None = None, root: int = 0, num_bins: int = 32, alpha: int = 15,
+        beta: int = 18, parents_out=None, stats: bool = False):
+    """nw::graph::bfs(out_graph, in_graph, root, num_bins, alpha, beta).
+
+    `in_graph` must be the registration that holds the transpose; the C ABI
+    registers out/in as one pair, so pass the same Graph (or None).
+    `num_bins` is accepted for signature compatibility; the device bins by
+    degree.  Returns the parents as a numpy uint32 array (and the Stats).
+    """
+    if in_graph is not None and in_graph is not out_graph:
+        raise ValueError("register the out/in pair as one Graph (Graph.from_csr(off, cols, in_off, in_cols))")
+    if num_bins <= 0:
+        raise ValueError("num_bins must be positive")
+    parents = parents_out if parents_out is not None else np.empty(out_graph.n, np.uint32)
+    s = Stats()
+    check(lib.nwg_bfs(out_graph.h, int(root), alpha, beta, _ptr(parents), None, C.byref(s) if stats else None))
+    return (parents, s) if stats else parents
+
+
+def bfs_device(g: Graph, root: int, parents_dev, alpha: int = 15, beta: int = 18, stats: bool = False):
+    """Synchronous traversal writing parents to a device array (torch tensor
+    or pointer) without a host copy."""
+    s = Stats()
+    check(lib.nwg_bfs(g.h, int(root), alpha, beta, None, _ptr(parents_dev), C.byref(s) if stats else None))
+    return s if stats else None
+
+
+def bfs_serial(graph: Graph, root: int, stats: bool = False):
+    """nw::graph::bfs(graph, root): top-down only, out-edges only."""
+    parents = np.empty(graph.n, np.uint32)
+    s = Stats()
+    check(lib.nwg_bfs_topdown(graph.h, int(root), _ptr(parents), None, C.byref(s) if stats else None))
+    return (parents, s) if stats else parents
+
+
+def depths_from_parents(parents: np.ndarray, root: int) -> np.ndarray:
+    """Depth of every vertex in the parent tree (NULL_VERTEX where unreached),
+    computed level by level with numpy.  Raises ValueError if the parents do
+    not form a tree rooted at `root`."""
+    parents = np.asarray(parents, dtype=np.uint32)
+    n = parents.size
+    depth = np.full(n, NULL_VERTEX, np.uint32)
+    if parents[root] != root:
+        raise ValueError("root is not its own parent")
+    depth[root] = 0
+    reached = parents != NULL_VERTEX
+    if np.any(parents[reached] >= n):
+        raise ValueError("parent id out of range")
+    pending = np.flatnonzero(reached)
+    pending = pending[pending != root]
+    d = 0
+    while pending.size:
+        par = parents[pending]
+        ready = depth[par] == d
+        if not np.any(ready):
+            raise ValueError("parents contain a cycle or a dangling chain")
+        depth[pending[ready]] = d + 1
+        pending = pending[~ready]
+        d += 1
+    return depth
+
+
+def bfs_verifier(off, cols, root, parents, in_off=None, in_cols=None) -> bool:
+    """nw::graph::BFSVerifier's checks (bfs.hpp:44-98) on host CSR arrays:
+    BFS depths from the out-graph; root self-parent at depth 0; every reached
+    u has parents[u] among in[u] one level closer; reachability agrees."""
+    off = np.asarray(off, np.uint64)
+    cols = np.asarray(cols, np.uint32)
+    if in_off is None:
+        in_off, in_cols = off, cols
+    n = off.size - 1
+    depth = np.full(n, NULL_VERTEX, np.int64)
+    depth[root] = 0
+    frontier = np.asarray([root], np.int64)
+    d = 0
+    deg = (off[1:] - off[:-1]).astype(np.int64)
+    while frontier.size:
+        starts = off[frontier].astype(np.int64)
+        lens = deg[frontier]
+        idx = np.repeat(starts - np.cumsum(lens) + lens, lens) + np.arange(lens.sum())
+        nbr = np.unique(cols[idx].astype(np.int64))
+        nbr = nbr[depth[nbr] == NULL_VERTEX]
+        d += 1
+        depth[nbr] = d
+        frontier = nbr
+    parents = np.asarray(parents, np.uint32)
+    reached_d = depth != NULL_VERTEX
+    reached_p = parents != NULL_VERTEX
+    if np.any(reached_d != reached_p):
+        return False
+    if parents[root] != root:
+        return False
+    us = np.flatnonzero(reached_p)
+    us = us[us != root]
+    if us.size == 0:
+        return True
+    pu = parents[us].astype(np.int64)
+    if np.any(depth[pu] != depth[us] - 1):
+        return False
+    # parents[u] must be an in-neighbour of u
+    in_off = np.asarray(in_off, np.uint64)
+    in_cols = np.asarray(in_cols, np.uint32)
+    ideg = (in_off[1:] - in_off[:-1]).astype(np.int64)
+    lens = ideg[us]
+    starts = in_off[us].astype(np.int64)
+    idx = np.repeat(starts - np.cumsum(lens) + lens, lens) + np.arange(lens.sum())
+    owner = np.repeat(np.arange(us.size), lens)
+    hit = np.zeros(us.size, bool)
+    match = in_cols[idx].astype(np.int64) == pu[owner]
+    hit[owner[match]] = True
+    return bool(hit.all())

@@ -1,0 +1,225 @@
+"""Parity of the CUDA direction-optimizing BFS with the oracle.
+
+Bar (bit-exact, all integer): per-vertex depths equal the reference's, the
+reached set is identical, the parents pass BFSVerifier's rules (checked by
+the C restatement, the numpy restatement, and the reference's own
+BFSVerifier when oracle/_ref is built), and the device's per-step direction
+decisions equal the restatement's (bfs.hpp:186,229,241).
+"""
+import numpy as np
+import pytest
+
+from oracle import graphgen as gg
+
+pytestmark = pytest.mark.gpu
+
+NULL = 0xFFFFFFFF
+
+
+def _check(nwg, port, reference, off, cols, root, parents, stats, in_off=None, in_cols=None, want_depths=None,
+           want_dir=None, want_found=None, numpy_verifier=True):
+    n = off.size - 1
+    depths = nwg.depths_from_parents(parents, int(root))
+    if want_depths is None:
+        want_depths = port.depths(off, cols, int(root))
+    assert np.array_equal(depths, want_depths), "depths differ from the oracle"
+    assert np.array_equal(parents != NULL, want_depths != NULL), "reached set differs"
+    assert port.verify(off, cols, root, parents, in_off, in_cols)
+    if numpy_verifier:
+        assert nwg.bfs_verifier(off, cols, root, parents, in_off, in_cols)
+    if reference is not None:
+        g = reference.graph(off, cols, in_off, in_cols)
+        assert g.verify(int(root), parents), "reference BFSVerifier rejected the device parents"
+        g.close()
+    if stats is not None:
+        tr = stats.trace()
+        if want_dir is None:
+            _, ptr = port.dobfs(off, cols, int(root), in_off, in_cols)
+            want_dir, want_found = ptr["dir"], ptr["found"]
+        k = min(len(want_dir), nwg.TRACE_CAP)
+        assert stats.status == 0
+        assert np.array_equal(tr["dir"][:k], np.asarray(want_dir)[:k]), "direction sequence differs"
+        assert np.array_equal(tr["found"][:k], np.asarray(want_found)[:k]), "per-step discoveries differ"
+        assert stats.reached == int(np.count_nonzero(want_depths != NULL))
+        assert stats.levels == int(want_depths[want_depths != NULL].max()) + 1
+
+
+def test_golden_fixtures(nwg, port, reference, golden):
+    for G in golden:
+        g = nwg.Graph.from_csr(G.off, G.cols, G.in_off, G.in_cols, validate=True)
+        for i, r in enumerate(G.roots):
+            parents, st = nwg.bfs(g, g, int(r), 32, 15, 18, stats=True)
+            _check(nwg, port, reference, G.off, G.cols, r, parents, st, G.in_off, G.in_cols,
+                   want_depths=G.depths[i], want_dir=G.trace_dir[i], want_found=G.trace_found[i])
+        g.release()
+
+
+def test_golden_u32_offsets(nwg, port, reference, golden):
+    """NWGraph's default adjacency<0> layout: uint32 offsets, widened on the device."""
+    for G in golden[:6]:
+        g = nwg.Graph.from_csr(G.off.astype(np.uint32), G.cols,
+                               None if G.in_off is None else G.in_off.astype(np.uint32), G.in_cols)
+        for i, r in enumerate(G.roots):
+            parents = nwg.bfs(g, g, int(r))
+            _check(nwg, port, reference, G.off, G.cols, r, parents, None, G.in_off, G.in_cols, want_depths=G.depths[i])
+        g.release()
+
+
+@pytest.mark.parametrize("scale", [12, 16])
+def test_rmat_host_graph(nwg, port, reference, scale):
+    off, cols = gg.rmat(scale, 16, seed=scale)
+    g = nwg.Graph.from_csr(off, cols)
+    for r in gg.roots(off, 6, seed=11):
+        parents, st = nwg.bfs(g, g, int(r), stats=True)
+        _check(nwg, port, reference, off, cols, r, parents, st)
+    g.release()
+
+
+def test_uniform_and_grid_host_graphs(nwg, port, reference):
+    for off, cols in (gg.uniform(1 << 14, 32, seed=3), gg.grid(128, 96, 1, seed=4), gg.grid(40, 40, 0, seed=1)):
+        g = nwg.Graph.from_csr(off, cols)
+        for r in gg.roots(off, 4, seed=5):
+            parents, st = nwg.bfs(g, g, int(r), stats=True)
+            _check(nwg, port, reference, off, cols, r, parents, st)
+        g.release()
+
+
+def test_directed_graph(nwg, port, reference):
+    """out != in: the in-graph is the transpose (bfs.hpp:216 reads in_graph[u])."""
+    rng = np.random.default_rng(1)
+    n = 5000
+    u = rng.integers(0, n, 40000).astype(np.uint64)
+    v = rng.integers(0, n, 40000).astype(np.uint64)
+    off, cols = gg.directed_csr(u, v, n)
+    in_off, in_cols = gg.transpose(off, cols, n)
+    g = nwg.Graph.from_csr(off, cols, in_off, in_cols, validate=True)
+    for r in gg.roots(off, 6, seed=9):
+        parents, st = nwg.bfs(g, g, int(r), stats=True)
+        _check(nwg, port, reference, off, cols, r, parents, st, in_off, in_cols)
+    g.release()
+
+
+def test_alpha_beta_variants(nwg, port, reference):
+    off, cols = gg.rmat(13, 16, seed=2)
+    g = nwg.Graph.from_csr(off, cols)
+    r = int(gg.roots(off, 1, seed=3)[0])
+    for alpha, beta in ((1, 1), (2, 100), (15, 18), (100, 2), (1000000, 18)):
+        parents, st = nwg.bfs(g, g, r, 32, alpha, beta, stats=True)
+        _, tr = port.dobfs(off, cols, r, alpha=alpha, beta=beta)
+        _check(nwg, port, reference, off, cols, r, parents, st, want_dir=tr["dir"], want_found=tr["found"])
+    g.release()
+
+
+def test_topdown_only(nwg, port):
+    off, cols = gg.rmat(12, 16, seed=4)
+    g = nwg.Graph.from_csr(off, cols)
+    for r in gg.roots(off, 3, seed=1):
+        parents, st = nwg.bfs_serial(g, int(r), stats=True)
+        assert np.array_equal(nwg.depths_from_parents(parents, int(r)), port.depths(off, cols, int(r)))
+        assert st.bu_steps == 0
+    g.release()
+
+
+def test_edge_cases(nwg, port):
+    # single vertex, no edges
+    g = nwg.Graph.from_csr(np.zeros(2, np.uint64), np.zeros(0, np.uint32))
+    assert nwg.bfs(g, g, 0).tolist() == [0]
+    g.release()
+    # isolated root among edges; self-loops and duplicates
+    off, cols = gg.directed_csr(np.array([1, 2, 2, 3, 3], np.uint64), np.array([2, 3, 3, 3, 1], np.uint64), 5)
+    g = nwg.Graph.from_csr(off, cols, *gg.transpose(off, cols, 5))
+    p = nwg.bfs(g, g, 0)
+    assert p.tolist() == [0, NULL, NULL, NULL, NULL]
+    p = nwg.bfs(g, g, 1)
+    assert nwg.depths_from_parents(p, 1).tolist() == [NULL, 0, 1, 2, NULL]
+    g.release()
+    # out-of-range root and bad alpha/beta are errors, not faults
+    off, cols = gg.rmat(8, 4, seed=1)
+    g = nwg.Graph.from_csr(off, cols)
+    with pytest.raises(nwg.NwgError) as e:
+        nwg.bfs(g, g, g.n)
+    assert e.value.code == nwg.NWG_EINVAL
+    with pytest.raises(nwg.NwgError):
+        nwg.bfs(g, g, 0, 32, 0, 18)
+    g.release()
+    # malformed CSR is rejected on the host before upload
+    with pytest.raises(nwg.NwgError) as e:
+        nwg.Graph.from_csr(np.array([0, 1, 2], np.uint64), np.array([1, 7], np.uint32), validate=True)
+    assert e.value.code == nwg.NWG_EINVAL
+    with pytest.raises(nwg.NwgError):
+        nwg.Graph.from_csr(np.array([0, 2, 1], np.uint64), np.array([1, 0], np.uint32), validate=True)
+
+
+def test_device_generators_match_numpy(nwg):
+    cases = [
+        (lambda: nwg.Graph.rmat(12, 16, seed=5), lambda: gg.rmat(12, 16, seed=5)),
+        (lambda: nwg.Graph.rmat(11, 8, seed=77), lambda: gg.rmat(11, 8, seed=77)),
+        (lambda: nwg.Graph.uniform(3000, 12, seed=6), lambda: gg.uniform(3000, 12, seed=6)),
+        (lambda: nwg.Graph.grid(70, 33, 1, seed=8), lambda: gg.grid(70, 33, 1, seed=8)),
+    ]
+    for mk_dev, mk_host in cases:
+        g = mk_dev()
+        off, cols = g.csr()
+        hoff, hcols = mk_host()
+        assert np.array_equal(off, hoff)
+        assert np.array_equal(cols, hcols)
+        assert np.array_equal(g.roots(16, seed=3), gg.roots(hoff, 16, seed=3))
+        g.release()
+
+
+def test_async_workspaces(nwg, port):
+    import torch
+
+    off, cols = gg.rmat(14, 16, seed=9)
+    g = nwg.Graph.from_csr(off, cols)
+    roots = gg.roots(off, 4, seed=2)
+    ws = [g.workspace() for _ in range(2)]
+    streams = [torch.cuda.Stream() for _ in range(2)]
+    outs = [torch.empty(g.n, dtype=torch.int32, device="cuda") for _ in range(2)]
+    for k in range(0, roots.size, 2):
+        for j in range(2):
+            ws[j].bfs_async(int(roots[k + j]), outs[j], streams[j].cuda_stream)
+        torch.cuda.synchronize()
+        for j in range(2):
+            p = outs[j].cpu().numpy().view(np.uint32)
+            r = int(roots[k + j])
+            assert np.array_equal(nwg.depths_from_parents(p, r), port.depths(off, cols, r))
+            assert ws[j].stats().status == 0
+    for w in ws:
+        w.close()
+    g.release()
+
+
+def test_rmat20_device_graph(nwg, port):
+    g = nwg.Graph.rmat(20, 16, seed=1)
+    off, cols = g.csr()
+    for r in g.roots(3, seed=27491095):
+        parents, st = nwg.bfs(g, g, int(r), stats=True)
+        _check(nwg, port, None, off, cols, r, parents, st)
+        import torch
+
+        dev = torch.empty(g.n, dtype=torch.int32, device="cuda")
+        nwg.bfs_device(g, int(r), dev)
+        e, v = g.component_edges(dev)
+        reached = parents != NULL
+        assert v == int(reached.sum())
+        assert e == int((off[1:] - off[:-1])[reached].sum())
+    g.release()
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("kind", ["rmat24", "uniform24", "grid4096"])
+def test_full_size(nwg, port, kind):
+    """The sizes the throughput figures are quoted on; depths bit-exact vs a
+    serial BFS of the same CSR copied back to the host."""
+    if kind == "rmat24":
+        g = nwg.Graph.rmat(24, 16, seed=1)
+    elif kind == "uniform24":
+        g = nwg.Graph.uniform(1 << 24, 32, seed=1)
+    else:
+        g = nwg.Graph.grid(4096, 4096, 1, seed=1)
+    off, cols = g.csr()
+    for r in g.roots(2, seed=27491095):
+        parents, st = nwg.bfs(g, g, int(r), stats=True)
+        _check(nwg, port, None, off, cols, r, parents, st, numpy_verifier=False)
+    g.release()
