@@ -277,15 +277,16 @@ def main():
     n_r = np.asarray(n_r, np.float64)
 
     if args.profile_one:
-        with torch.cuda.stream(stream):
-            ws.bfs_async(int(roots[0]), parents, stream.cuda_stream)
-        stream.synchronize()
+        # the same kernels launched one at a time from the host (ncu cannot
+        # profile kernels inside a CUDA graph with conditional nodes)
+        nwg.bfs_stepped(g, int(roots[0]), parents)
+        torch.cuda.synchronize()
         torch.cuda.nvtx.range_push("nwg_profile")
-        with torch.cuda.stream(stream):
-            ws.bfs_async(int(roots[0]), parents, stream.cuda_stream)
-        stream.synchronize()
+        st = nwg.bfs_stepped(g, int(roots[0]), parents)
+        torch.cuda.synchronize()
         torch.cuda.nvtx.range_pop()
-        print(json.dumps({"profile_one": True, "root": int(roots[0]), "n": n, "m": m}))
+        print(json.dumps({"profile_one": True, "root": int(roots[0]), "n": n, "m": m, "steps": st.steps,
+                          "trace_dir": st.trace()["dir"].tolist()}))
         return
 
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in roots]

@@ -63,6 +63,12 @@ typedef struct {
   uint8_t trace_dir[NWG_TRACE_CAP];
   uint64_t trace_frontier[NWG_TRACE_CAP];
   uint64_t trace_found[NWG_TRACE_CAP];
+  /* device clock (%globaltimer, ns since the traversal's init kernel) when
+   * the level loop consumed each step's result; first_decide_ns is the first
+   * decision.  Step i took trace_end_ns[i] - trace_end_ns[i-1] (i = 0:
+   * minus first_decide_ns), launch gaps included. */
+  uint64_t trace_end_ns[NWG_TRACE_CAP];
+  uint64_t first_decide_ns;
 } nwg_bfs_stats;
 
 /* Library version string. */
@@ -114,6 +120,12 @@ int nwg_bfs_async(nwg_bfs_ws ws, uint32_t root, int alpha, int beta, uint32_t* p
 
 /* Statistics of the workspace's last traversal; synchronises with it. */
 int nwg_ws_stats(nwg_bfs_ws ws, nwg_bfs_stats* stats);
+
+/* nwg_bfs with the level loop driven from the host: the same kernels
+ * launched one at a time, the decision read back after every step.  For
+ * profilers (ncu cannot profile the kernels of a CUDA graph with
+ * conditional nodes one by one) and debugging; slower than nwg_bfs. */
+int nwg_bfs_stepped(nwg_graph g, uint32_t root, int alpha, int beta, uint32_t* parents_dev, nwg_bfs_stats* stats);
 
 /* Top-down-only BFS (no in-graph needed); replaces the one-graph
  * nw::graph::bfs(graph, root) (algorithms/bfs.hpp:110-140). */

@@ -37,7 +37,7 @@ REG_VALIDATE = 0x2
 EXPORTED = (
     "nwg_version", "nwg_last_error", "nwg_graph_register", "nwg_graph_register_u32off", "nwg_graph_release",
     "nwg_graph_info", "nwg_bfs", "nwg_ws_create", "nwg_ws_destroy", "nwg_bfs_async", "nwg_ws_stats",
-    "nwg_bfs_topdown", "nwg_component_edges", "nwg_graph_copy_csr", "nwg_gen_rmat", "nwg_gen_uniform",
+    "nwg_bfs_topdown", "nwg_bfs_stepped", "nwg_component_edges", "nwg_graph_copy_csr", "nwg_gen_rmat", "nwg_gen_uniform",
     "nwg_gen_grid", "nwg_pick_roots",
 )
 
@@ -54,6 +54,7 @@ class Stats(C.Structure):
         ("bu_steps", C.c_uint32), ("b2q_steps", C.c_uint32), ("reached", C.c_uint64), ("device_ms", C.c_float),
         ("trace_len", C.c_uint32), ("trace_dir", C.c_uint8 * TRACE_CAP),
         ("trace_frontier", C.c_uint64 * TRACE_CAP), ("trace_found", C.c_uint64 * TRACE_CAP),
+        ("trace_end_ns", C.c_uint64 * TRACE_CAP), ("first_decide_ns", C.c_uint64),
     ]
 
     def trace(self):
@@ -62,7 +63,13 @@ class Stats(C.Structure):
             "dir": np.frombuffer(bytes(self.trace_dir), np.uint8)[:k].copy(),
             "frontier": np.ctypeslib.as_array(self.trace_frontier)[:k].copy(),
             "found": np.ctypeslib.as_array(self.trace_found)[:k].copy(),
+            "end_ns": np.ctypeslib.as_array(self.trace_end_ns)[:k].copy(),
         }
+
+    def step_ns(self):
+        """Device time of each step (launch gaps included), from the trace."""
+        end = np.ctypeslib.as_array(self.trace_end_ns)[: self.trace_len].astype(np.int64)
+        return np.diff(np.concatenate([[int(self.first_decide_ns)], end]))
 
 
 _vp = C.c_void_p
@@ -71,7 +78,7 @@ _u32, _u64, _int = C.c_uint32, C.c_uint64, C.c_int
 
 def _load():
     if not os.path.exists(LIB_PATH):
-        raise ImportError(f"{LIB_PATH} is not built; run `python -m nwgr_b200.build` (nvcc, sm_100a)")
+        raise ImportError(f"{LIB_PATH} is not built; run `python nwgr_b200/build.py` (nvcc, sm_100a)")
     lib = C.CDLL(LIB_PATH)
     sig = {
         "nwg_version": (C.c_char_p, []),
@@ -86,6 +93,7 @@ def _load():
         "nwg_bfs_async": (_int, [_vp, _u32, _int, _int, _vp, _vp]),
         "nwg_ws_stats": (_int, [_vp, C.POINTER(Stats)]),
         "nwg_bfs_topdown": (_int, [_vp, _u32, _vp, _vp, C.POINTER(Stats)]),
+        "nwg_bfs_stepped": (_int, [_vp, _u32, _int, _int, _vp, C.POINTER(Stats)]),
         "nwg_component_edges": (_int, [_vp, _vp, C.POINTER(_u64), C.POINTER(_u64)]),
         "nwg_graph_copy_csr": (_int, [_vp, _vp, _vp, _vp, _vp]),
         "nwg_gen_rmat": (_int, [_u32, _u32, _u64, _u32, _u32, _u32, C.POINTER(_vp)]),
@@ -274,6 +282,14 @@ def bfs_device(g: Graph, root: int, parents_dev, alpha: int = 15, beta: int = 18
     s = Stats()
     check(lib.nwg_bfs(g.h, int(root), alpha, beta, None, _ptr(parents_dev), C.byref(s) if stats else None))
     return s if stats else None
+
+
+def bfs_stepped(g: Graph, root: int, parents_dev=None, alpha: int = 15, beta: int = 18):
+    """The same traversal with the level loop driven from the host, one
+    kernel launch at a time (for profilers).  Returns the Stats."""
+    s = Stats()
+    check(lib.nwg_bfs_stepped(g.h, int(root), alpha, beta, _ptr(parents_dev), C.byref(s)))
+    return s
 
 
 def bfs_serial(graph: Graph, root: int, stats: bool = False):

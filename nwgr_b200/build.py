@@ -1,7 +1,10 @@
 """Build recipe of libnwgr_b200.so (in-tree, sm_100a only).
 
-    python -m nwgr_b200.build            # build if sources are newer
-    python -m nwgr_b200.build --force
+    python nwgr_b200/build.py            # build if sources are newer
+    python nwgr_b200/build.py --force
+
+Run it as a script (or load it by path, as __graft_entry__.build() and the
+test suite do): importing the nwgr_b200 package loads the library it builds.
 
 The library is compiled straight with nvcc for sm_100a (no PTX for other
 architectures, no JIT cache): every .cu under nwgr_b200/csrc goes into one
@@ -62,3 +65,4 @@ def build(force: bool = False, verbose: bool = False) -> str:
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose=True)
     print(LIB)
+

@@ -234,7 +234,7 @@ int bfs_sync(GraphDev* g, uint32_t root, int alpha, int beta, uint32_t* parents_
   NWG_CUDA_TRY(cudaEventRecord(ws->ev1, ws->stream));
   if (parents_host)
     NWG_CUDA_TRY(cudaMemcpyAsync(parents_host, dst, g->n * sizeof(uint32_t), cudaMemcpyDeviceToHost, ws->stream));
-  const size_t ctrl_bytes = stats ? sizeof(Ctrl) : offsetof(Ctrl, trace_dir);
+  const size_t ctrl_bytes = stats ? sizeof(Ctrl) : sizeof(CtrlHdr);
   NWG_CUDA_TRY(cudaMemcpyAsync(ws->ctrl_host, ws->ctrl, ctrl_bytes, cudaMemcpyDeviceToHost, ws->stream));
   NWG_CUDA_TRY(cudaStreamSynchronize(ws->stream));
   const Ctrl& c = *ws->ctrl_host;
@@ -244,7 +244,7 @@ int bfs_sync(GraphDev* g, uint32_t root, int alpha, int beta, uint32_t* parents_
     cudaEventElapsedTime(&ms, ws->ev0, ws->ev1);
     stats->device_ms = ms;
   }
-  if (c.status != 0) return set_error(c.status, "device traversal reported status " + std::to_string(c.status));
+  if (c.h.status != 0) return set_error(c.h.status, "device traversal reported status " + std::to_string(c.h.status));
   return NWG_OK;
 }
 
@@ -334,6 +334,34 @@ NWG_API int nwg_bfs_topdown(nwg_graph h, uint32_t root, uint32_t* parents_host, 
   NWG_GUARD_BEGIN
   if (!h) return set_error(NWG_EINVAL, "NULL graph");
   return bfs_sync(reinterpret_cast<GraphDev*>(h), root, 15, 18, parents_host, parents_dev, stats, true);
+  NWG_GUARD_END
+}
+
+NWG_API int nwg_bfs_stepped(nwg_graph h, uint32_t root, int alpha, int beta, uint32_t* parents_dev,
+                            nwg_bfs_stats* stats) {
+  NWG_GUARD_BEGIN
+  if (!h) return set_error(NWG_EINVAL, "NULL graph");
+  auto*                       g = reinterpret_cast<GraphDev*>(h);
+  std::lock_guard<std::mutex> lk(g->mu);
+  DeviceGuard                 dg(g->device);
+  Workspace*                  ws = nullptr;
+  int                         rc = get_default_ws(g, &ws);
+  if (rc) return rc;
+  NWG_CUDA_TRY(cudaEventRecord(ws->ev0, ws->stream));
+  rc = ws_launch_stepped(ws, root, alpha, beta, parents_dev, ws->stream);
+  if (rc) return rc;
+  NWG_CUDA_TRY(cudaEventRecord(ws->ev1, ws->stream));
+  NWG_CUDA_TRY(cudaMemcpyAsync(ws->ctrl_host, ws->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, ws->stream));
+  NWG_CUDA_TRY(cudaStreamSynchronize(ws->stream));
+  if (stats) {
+    fill_stats(*ws->ctrl_host, stats);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ws->ev0, ws->ev1);
+    stats->device_ms = ms;
+  }
+  const int st = ws->ctrl_host->h.status;
+  if (st != 0) return set_error(st, "device traversal reported status " + std::to_string(st));
+  return NWG_OK;
   NWG_GUARD_END
 }
 

@@ -3,7 +3,7 @@
 // Restates nw::graph::bfs(out, in, root, num_bins, alpha, beta)
 // (include/nwgraph/algorithms/bfs.hpp:160-311 in NWGraph) as a CUDA graph:
 //
-//   k_init ──► WHILE(h_loop) { k_decide ──► SWITCH(h_switch) { k_td | k_bu | k_b2q } }
+//   k_init ──► WHILE(h_loop) { k_decide ──► SWITCH(h_switch) { k_td | k_bu | k_b2q | k_td(small grid) } }
 //
 // k_decide is a one-thread kernel that reproduces the reference's integer
 // switch rules exactly (scout_count > edges_to_check / alpha selects
@@ -13,7 +13,7 @@
 // finds nothing, bfs.hpp:231-233) and sets the graph's conditional handles,
 // so no level makes a host round trip.
 //
-// Device state (HBM, all uint32 words):
+// Device state (HBM):
 //   parents[n]   output; null = 0xFFFFFFFF
 //   V[n/32]      visited bitmap.  The top-down step sets a vertex's bit with
 //                atomicOr when it claims it (this is the queue->bitmap
@@ -23,8 +23,9 @@
 //   C0/C1[n/32]  discoveries of the latest bottom-up pulls (bfs.hpp:205-229's
 //                front/curr pair).
 //   Z[n/32]      vertices with no in-edges, never candidates of a pull.
-//   q[2][4][..]  frontier queues, binned by out-degree (thread-gather, warp,
-//                CTA, grid) instead of the reference's u % 32 bins.
+//   qs[2], qc[2] frontier queues: small-degree vertex ids, and 256-edge
+//                chunks of every other vertex (instead of the reference's
+//                u % 32 bins).
 //
 // Bottom-up front: the first pull of a phase uses V itself as the front
 // bitmap.  V holds the frontier plus all earlier levels; an earlier-level
@@ -41,13 +42,31 @@
 namespace nwg {
 namespace {
 
-constexpr int kThreads = 256;
-constexpr int kBuProbe = 4;  // sequential in-edge probes per lane before the warp helps
+constexpr int kThreads     = 256;
+constexpr int kWarps       = kThreads / 32;
+constexpr int kBuProbe     = 4;   // in-edges a lane tests per round (independent loads)
+constexpr int kBuLane      = 32;  // in-edges a lane scans alone before the warp helps
+constexpr int kTileWords   = 32;  // bitmap words per warp tile of the bitmap->queue pass (1024 vertices)
+constexpr int kBuTileWords = 8;   // bitmap words per pull tile (256 vertices)
+constexpr int kSmallBlocks = 64;  // grid of the small-frontier top-down branch
+constexpr int kVisit       = 4;   // edges a lane claims per batch
+constexpr int kTdPerSm     = 3;   // k_td blocks per SM (80 registers per thread: 3 x 256 threads fill an SM)
 
-__device__ __forceinline__ unsigned lanemask_lt() {
-  unsigned m;
-  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-  return m;
+__device__ __forceinline__ unsigned long long globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_incl_scan(T v) {
+  const unsigned lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const T x = __shfl_up_sync(kFullMask, v, o);
+    if ((int)lane >= o) v += x;
+  }
+  return v;
 }
 
 template <typename T>
@@ -65,6 +84,362 @@ __device__ __forceinline__ T block_sum(T v) {
     for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(kFullMask, t, o);
   }
   return t;  // valid in thread 0
+}
+
+__host__ __device__ __forceinline__ uint64_t chunks_of(uint64_t deg, const Thresholds& t) {
+  return (deg + t.chunk - 1) >> t.chunk_shift;
+}
+
+constexpr uint64_t kLaneChunks = 8;  // a lane writes up to this many chunk entries of one vertex itself
+
+// ---------------------------------------------------------------------------
+// Appending discovered vertices to the next queue buffer `qi`.
+//
+// A lane holds K vertices (mask bit k set = v[k] valid) with their
+// out-degrees.  Small-degree vertices take one small-queue slot, the others
+// chunks_of(d) chunk-queue slots.  Space in both queues is reserved with ONE
+// 64-bit atomicAdd on the packed position counter qpos[qi] per warp
+// (append_warp, a warp's buffer ran full) or per block (append_block, the
+// end-of-kernel flush): same-address atomics serialise in L2, so their
+// number, not the bytes written, bounds a step that discovers millions of
+// vertices.  The chunk entries of each chunked vertex are written by the
+// whole warp, 32 at a time.
+template <int K>
+__device__ __forceinline__ void count_entries(const DobfsParams& p, const uint64_t (&d)[K], uint32_t mask,
+                                              uint32_t& ns, uint32_t& nch, uint32_t& nb) {
+  ns = nch = nb = 0;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    if (mask & (1u << k)) {
+      if (d[k] < p.th.warp_min) {
+        ++ns;
+      } else {
+        ++nb;
+        nch += (uint32_t)chunks_of(d[k], p.th);
+      }
+    }
+  }
+}
+
+// All 32 lanes of the warp must call.  Small entries and the chunk entries
+// of vertices with at most kLaneChunks chunks are written by their own lane;
+// the chunk entries of hubs are written by the whole warp, 32 at a time.
+template <int K>
+__device__ __forceinline__ void write_entries(const DobfsParams& p, uint32_t qi, const uint32_t (&v)[K],
+                                              const uint64_t (&d)[K], uint32_t mask, uint64_t spos, uint64_t cpos,
+                                              uint32_t nch) {
+  CtrlHdr*        c    = &p.ctrl->h;
+  const unsigned  lane = threadIdx.x & 31;
+  uint32_t* const qs   = p.qs[qi];
+  uint64_t* const qc   = p.qc[qi];
+  const uint64_t  c0   = cpos;
+  bool            hub  = false;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    if (!(mask & (1u << k))) continue;
+    if (d[k] < p.th.warp_min) {
+      if (spos < p.qs_cap) {
+        qs[spos] = v[k];
+      } else {
+        c->status = NWG_EOVERFLOW;
+      }
+      ++spos;
+    } else {
+      const uint64_t nc = chunks_of(d[k], p.th);
+      if (nc <= kLaneChunks) {
+        for (uint64_t j = 0; j < nc; ++j) {
+          if (cpos + j < p.qc_cap) {
+            qc[cpos + j] = ((uint64_t)v[k] << 32) | j;
+          } else {
+            c->status = NWG_EOVERFLOW;
+          }
+        }
+      } else {
+        hub = true;
+      }
+      cpos += nc;
+    }
+  }
+  unsigned todo = __ballot_sync(kFullMask, hub);
+  while (todo) {
+    const int src = __ffs(todo) - 1;
+    todo &= todo - 1;
+    uint64_t pos = __shfl_sync(kFullMask, c0, src);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const unsigned valid = __shfl_sync(kFullMask, (mask >> k) & 1u, src);
+      const uint64_t dk    = __shfl_sync(kFullMask, d[k], src);
+      if (valid && dk >= p.th.warp_min) {
+        const uint64_t nc = chunks_of(dk, p.th);
+        if (nc > kLaneChunks) {
+          const uint32_t vk = __shfl_sync(kFullMask, v[k], src);
+          for (uint64_t j = lane; j < nc; j += 32) {
+            if (pos + j < p.qc_cap) {
+              qc[pos + j] = ((uint64_t)vk << 32) | j;
+            } else {
+              c->status = NWG_EOVERFLOW;
+            }
+          }
+        }
+        pos += nc;
+      }
+    }
+  }
+  (void)nch;
+}
+
+template <int K>
+__device__ __forceinline__ void append_warp(const DobfsParams& p, uint32_t qi, const uint32_t (&v)[K],
+                                            const uint64_t (&d)[K], uint32_t mask, uint32_t& nbig) {
+  uint32_t ns, nch, nb;
+  count_entries<K>(p, d, mask, ns, nch, nb);
+  nbig += nb;
+  const unsigned long long mine = (unsigned long long)ns | ((unsigned long long)nch << 32);
+  const unsigned long long incl = warp_incl_scan(mine);
+  const unsigned long long tot  = __shfl_sync(kFullMask, incl, 31);
+  if (tot == 0) return;
+  unsigned long long base = 0;
+  if ((threadIdx.x & 31) == 31) base = atomicAdd(&p.ctrl->h.qpos[qi], tot);
+  base                          = __shfl_sync(kFullMask, base, 31);
+  const unsigned long long excl = incl - mine;
+  write_entries<K>(p, qi, v, d, mask, (base & 0xFFFFFFFFull) + (excl & 0xFFFFFFFFull), (base >> 32) + (excl >> 32),
+                   nch);
+}
+
+// Exclusive block-wide scan of a 64-bit value; all threads call.
+__device__ __forceinline__ unsigned long long block_excl_scan(unsigned long long x, unsigned long long& total) {
+  __shared__ unsigned long long s_w[kWarps];
+  __shared__ unsigned long long s_p[kWarps];
+  const unsigned                lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const unsigned long long      inc  = warp_incl_scan(x);
+  if (lane == 31) s_w[wib] = inc;
+  __syncthreads();
+  if (wib == 0) {
+    const unsigned long long t  = lane < kWarps ? s_w[lane] : 0ull;
+    const unsigned long long ti = warp_incl_scan(t);
+    if (lane < kWarps) s_p[lane] = ti;
+  }
+  __syncthreads();
+  total                         = s_p[kWarps - 1];
+  const unsigned long long excl = (wib ? s_p[wib - 1] : 0ull) + inc - x;
+  __syncthreads();
+  return excl;
+}
+
+template <int K>
+__device__ __forceinline__ void append_block(const DobfsParams& p, uint32_t qi, const uint32_t (&v)[K],
+                                             const uint64_t (&d)[K], uint32_t mask, uint32_t& nbig) {
+  __shared__ unsigned long long s_base;
+  uint32_t                      ns, nch, nb;
+  count_entries<K>(p, d, mask, ns, nch, nb);
+  nbig += nb;
+  const unsigned long long mine = (unsigned long long)ns | ((unsigned long long)nch << 32);
+  unsigned long long       tot  = 0;
+  const unsigned long long excl = block_excl_scan(mine, tot);
+  if (tot == 0) return;  // block-uniform
+  if (threadIdx.x == 0) s_base = atomicAdd(&p.ctrl->h.qpos[qi], tot);
+  __syncthreads();
+  const unsigned long long base = s_base;
+  write_entries<K>(p, qi, v, d, mask, (base & 0xFFFFFFFFull) + (excl & 0xFFFFFFFFull), (base >> 32) + (excl >> 32),
+                   nch);
+  __syncthreads();
+}
+
+// Per-warp shared state of the top-down step: the ranges of the current
+// gather group (owner search) and a buffer of claimed vertices whose degree
+// lookup and queue append are done in bulk.
+constexpr int kWinBuf = 256;
+struct TdWarp {
+  uint32_t vexcl[33];  // exclusive prefix of the ranges' aligned-body vector counts; [32] = total
+  uint32_t sexcl[33];  // exclusive prefix of the ranges' head + tail edge counts; [32] = total
+  uint32_t u[32];      // source vertex of each range
+  uint32_t nhead[32];  // head length (edges before the first 16-byte boundary)
+  uint64_t lo[32];     // first edge of the range
+  uint64_t al[32];     // first edge of the aligned body
+  uint64_t ah[32];     // end of the aligned body (= start of the tail)
+  uint32_t win[kWinBuf];
+};
+
+// A warp's winner buffer ran full: degree lookup and append of its entries
+// (all 32 lanes call).
+__device__ __forceinline__ void flush_winners(const DobfsParams& p, TdWarp& tw, uint32_t& wcnt, uint32_t nxt,
+                                              unsigned long long& scout, uint32_t& nbig) {
+  const unsigned lane = threadIdx.x & 31;
+  __syncwarp();
+  for (uint32_t r = 0; r < wcnt; r += 32 * kVisit) {
+    uint32_t v[kVisit];
+    uint64_t d[kVisit];
+    uint32_t mask = 0;
+#pragma unroll
+    for (int k = 0; k < kVisit; ++k) {
+      const uint32_t i = r + k * 32 + lane;
+      v[k]             = 0;
+      d[k]             = 0;
+      if (i < wcnt) {
+        v[k] = tw.win[i];
+        mask |= 1u << k;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kVisit; ++k)
+      if (mask & (1u << k)) d[k] = p.off[v[k] + 1] - p.off[v[k]];
+#pragma unroll
+    for (int k = 0; k < kVisit; ++k) scout += d[k];
+    append_warp<kVisit>(p, nxt, v, d, mask, nbig);
+  }
+  wcnt = 0;
+  __syncwarp();
+}
+
+// End of a step: every warp's remaining buffered winners are appended with
+// one reservation for the whole block.  All threads of the block call.
+__device__ __forceinline__ void flush_block(const DobfsParams& p, TdWarp* tws, uint32_t wcnt, uint32_t nxt,
+                                            unsigned long long& scout, uint32_t& nbig, bool count_scout) {
+  __shared__ uint32_t s_cnt[kWarps];
+  if ((threadIdx.x & 31) == 0) s_cnt[threadIdx.x >> 5] = wcnt;
+  __syncthreads();
+  uint32_t v[kWarps];
+  uint64_t d[kWarps];
+  uint32_t mask = 0;
+#pragma unroll
+  for (int w = 0; w < kWarps; ++w) {
+    v[w] = 0;
+    d[w] = 0;
+    if (threadIdx.x < s_cnt[w]) {
+      v[w] = tws[w].win[threadIdx.x];
+      mask |= 1u << w;
+    }
+  }
+#pragma unroll
+  for (int w = 0; w < kWarps; ++w)
+    if (mask & (1u << w)) d[w] = p.off[v[w] + 1] - p.off[v[w]];
+  if (count_scout) {
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) scout += d[w];
+  }
+  append_block<kWarps>(p, nxt, v, d, mask, nbig);
+}
+
+// One batch of top-down edge tests (bfs.hpp:280-289): lane edges u[k] -> v[k]
+// for the valid k.  Every V word is read first (independent loads, through L1:
+// bits only ever go from 0 to 1, so a stale word can only cost an extra
+// atomic, never a wrong claim), then the unvisited ones are claimed with
+// atomicOr (all issued before any result is used).  A claim's winner writes parents[v] = u (the reference's CAS
+// winner) and is buffered; scout and the next queue are updated when the
+// buffer is flushed.  All 32 lanes must call.
+__device__ __forceinline__ void visit_batch(const DobfsParams& p, uint32_t* __restrict__ parents, uint32_t nxt,
+                                            const uint32_t (&u)[kVisit], const uint32_t (&v)[kVisit], uint32_t valid,
+                                            TdWarp& tw, uint32_t& wcnt, unsigned long long& scout, uint32_t& nbig) {
+  uint32_t w[kVisit];
+#pragma unroll
+  for (int k = 0; k < kVisit; ++k) w[k] = (valid & (1u << k)) ? p.V[v[k] >> 5] : ~0u;
+  uint32_t old[kVisit];
+  uint32_t try_mask = 0;
+#pragma unroll
+  for (int k = 0; k < kVisit; ++k) {
+    const uint32_t bit = 1u << (v[k] & 31);
+    old[k]             = ~0u;
+    if (!(w[k] & bit)) {
+      old[k] = atomicOr(p.V + (v[k] >> 5), bit);
+      try_mask |= 1u << k;
+    }
+  }
+  uint32_t win = 0;
+#pragma unroll
+  for (int k = 0; k < kVisit; ++k)
+    if ((try_mask & (1u << k)) && !(old[k] & (1u << (v[k] & 31)))) win |= 1u << k;
+  const uint32_t cnt = __popc(win);
+  const uint32_t inc = warp_incl_scan(cnt);
+  const uint32_t tot = __shfl_sync(kFullMask, inc, 31);
+  if (tot == 0) return;
+  uint32_t pos = wcnt + inc - cnt;
+#pragma unroll
+  for (int k = 0; k < kVisit; ++k) {
+    if (win & (1u << k)) {
+      parents[v[k]] = u[k];
+      tw.win[pos++] = v[k];
+    }
+  }
+  wcnt += tot;
+  if (wcnt > kWinBuf - 32 * kVisit) flush_winners(p, tw, wcnt, nxt, scout, nbig);
+}
+
+// Largest range index whose exclusive prefix (in `excl`) is <= e.
+__device__ __forceinline__ int owner_of(const uint32_t* excl, uint32_t e) {
+  int lo = 0;
+#pragma unroll
+  for (int s = 16; s >= 1; s >>= 1)
+    if (excl[lo + s] <= e) lo += s;
+  return lo;
+}
+
+// Expands up to 32 edge ranges at once (lane i holds range i: source u,
+// edges [lo, hi); lo == hi = none).  Each range splits into an unaligned head,
+// a 16-byte-aligned body and a tail.  The bodies of all ranges are flattened
+// by a warp scan and dealt out one 128-bit non-coherent load (4 edges of one
+// range) per lane per batch; the heads and tails (< 4 edges each) are dealt
+// out as scalar edges, kVisit per lane per batch.  A unit's range is found by
+// binary search over the prefix in shared memory.  All 32 lanes must call.
+__device__ __forceinline__ void gather_ranges(const DobfsParams& p, uint32_t* __restrict__ parents, uint32_t nxt,
+                                              uint32_t u, uint64_t lo, uint64_t hi, TdWarp& tw, uint32_t& wcnt,
+                                              unsigned long long& scout, uint32_t& nbig) {
+  const unsigned lane = threadIdx.x & 31;
+  const uint64_t al   = min(hi, (lo + 3) & ~(uint64_t)3);
+  const uint64_t ah   = max(al, hi & ~(uint64_t)3);
+  const uint32_t nvec = (uint32_t)((ah - al) >> 2);
+  const uint32_t nsc  = (uint32_t)((al - lo) + (hi - ah));
+  const uint32_t vinc = warp_incl_scan(nvec);
+  const uint32_t sinc = warp_incl_scan(nsc);
+  const uint32_t vtot = __shfl_sync(kFullMask, vinc, 31);
+  const uint32_t stot = __shfl_sync(kFullMask, sinc, 31);
+  if (vtot == 0 && stot == 0) return;
+  tw.vexcl[lane] = vinc - nvec;
+  tw.sexcl[lane] = sinc - nsc;
+  tw.u[lane]     = u;
+  tw.nhead[lane] = (uint32_t)(al - lo);
+  tw.lo[lane]    = lo;
+  tw.al[lane]    = al;
+  tw.ah[lane]    = ah;
+  if (lane == 31) {
+    tw.vexcl[32] = vtot;
+    tw.sexcl[32] = stot;
+  }
+  __syncwarp();
+  const uint4* col4 = reinterpret_cast<const uint4*>(p.col);
+  for (uint32_t j = 0; j < vtot; j += 32) {
+    const uint32_t e  = j + lane;
+    uint32_t       uu[kVisit] = {0, 0, 0, 0}, vv[kVisit] = {0, 0, 0, 0}, valid = 0;
+    if (e < vtot) {
+      const int   o = owner_of(tw.vexcl, e);
+      const uint4 x = __ldg(col4 + ((tw.al[o] >> 2) + (e - tw.vexcl[o])));
+      uu[0] = uu[1] = uu[2] = uu[3] = tw.u[o];
+      vv[0] = x.x;
+      vv[1] = x.y;
+      vv[2] = x.z;
+      vv[3] = x.w;
+      valid = 0xFu;
+    }
+    visit_batch(p, parents, nxt, uu, vv, valid, tw, wcnt, scout, nbig);
+  }
+  for (uint32_t j = 0; j < stot; j += 32 * kVisit) {
+    uint32_t uu[kVisit], vv[kVisit], valid = 0;
+#pragma unroll
+    for (int k = 0; k < kVisit; ++k) {
+      const uint32_t e = j + k * 32 + lane;
+      uu[k]            = 0;
+      vv[k]            = 0;
+      if (e < stot) {
+        const int      o = owner_of(tw.sexcl, e);
+        const uint32_t t = e - tw.sexcl[o];
+        const uint64_t i = t < tw.nhead[o] ? tw.lo[o] + t : tw.ah[o] + (t - tw.nhead[o]);
+        uu[k]            = tw.u[o];
+        vv[k]            = __ldg(p.col + i);
+        valid |= 1u << k;
+      }
+    }
+    visit_batch(p, parents, nxt, uu, vv, valid, tw, wcnt, scout, nbig);
+  }
+  __syncwarp();
 }
 
 // ---------------------------------------------------------------------------
@@ -99,7 +474,7 @@ __global__ void __launch_bounds__(kThreads) k_init(DobfsParams p, uint32_t root,
   for (uint64_t w = tid; w < p.nwords; w += stride) p.V[w] = (w == rw) ? (1u << (root & 31)) : 0u;
 
   if (tid == 0) {
-    Ctrl&          c   = *p.ctrl;
+    CtrlHdr&       c   = p.ctrl->h;
     const uint64_t deg = p.off[root + 1] - p.off[root];
     c.parents          = parents;
     c.root             = root;
@@ -112,10 +487,17 @@ __global__ void __launch_bounds__(kThreads) k_init(DobfsParams p, uint32_t root,
     c.old_awake        = 0;
     c.acc_scout        = 0;
     c.acc_awake        = 0;
-    for (int b = 0; b < kNumBins; ++b) c.qcount[0][b] = c.qcount[1][b] = 0;
-    const int b = degree_bin(deg, p.th);
-    p.q[0][b][0] = root;
-    c.qcount[0][b] = 1;
+    c.qpos[0] = c.qpos[1] = 0;
+    c.qbig[0] = c.qbig[1] = 0;
+    if (deg < p.th.warp_min) {
+      p.qs[0][0] = root;
+      c.qpos[0]  = 1;
+    } else {
+      const uint64_t nc = chunks_of(deg, p.th);
+      for (uint64_t j = 0; j < nc && j < p.qc_cap; ++j) p.qc[0][j] = ((uint64_t)root << 32) | j;
+      c.qpos[0] = nc << 32;
+      c.qbig[0] = 1;
+    }
     c.cur       = 0;
     c.bm        = 1;
     c.bu_mode   = 0;
@@ -125,48 +507,63 @@ __global__ void __launch_bounds__(kThreads) k_init(DobfsParams p, uint32_t root,
     c.td_steps  = 0;
     c.bu_steps  = 0;
     c.b2q_steps = 0;
-    c.status    = 0;
-    c.reached   = 1;
+    c.status      = 0;
+    c.pre_decided = 0;
+    p.ctrl->bar.count = 0;
+    p.ctrl->err       = 0;
+    c.reached     = 1;
+    c.t_start     = globaltimer();
     c.trace_len = 0;
     const uint64_t cap = 2 * n + 64;
     c.max_steps = cap > 0xFFFFFF00ull ? 0xFFFFFF00u : (uint32_t)cap;
   }
 }
 
-__device__ __forceinline__ uint64_t qsum(const Ctrl& c, uint32_t qi) {
-  uint64_t s = 0;
-#pragma unroll
-  for (int b = 0; b < kNumBins; ++b) s += c.qcount[qi][b];
-  return s;
+__device__ __forceinline__ uint64_t frontier_size(const CtrlHdr& c, uint32_t qi) {
+  return (c.qpos[qi] & 0xFFFFFFFFull) + c.qbig[qi];
 }
 
-__device__ __forceinline__ void trace_add(Ctrl& c, uint8_t dir, uint64_t frontier, uint64_t found) {
+__device__ __forceinline__ void trace_add(Ctrl* ctrl, CtrlHdr& c, uint8_t dir, uint64_t frontier, uint64_t found,
+                                          unsigned long long now) {
   if (c.trace_len < NWG_TRACE_CAP) {
-    c.trace_dir[c.trace_len]      = dir;
-    c.trace_frontier[c.trace_len] = frontier;
-    c.trace_found[c.trace_len]    = found;
+    ctrl->trace_dir[c.trace_len]      = dir;
+    ctrl->trace_frontier[c.trace_len] = frontier;
+    ctrl->trace_found[c.trace_len]    = found;
+    ctrl->trace_end_ns[c.trace_len]   = now - c.t_start;
     c.trace_len++;
   }
 }
 
 // ---------------------------------------------------------------------------
-// k_decide: one thread; consumes the previous action's counters and picks the
-// next action.  Every branch below cites the reference line it reproduces.
-__global__ void k_decide(DobfsParams p) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  Ctrl&          c    = *p.ctrl;
+// decide_core: one thread; consumes the previous action's counters and picks
+// the next action.  Every branch below cites the reference line it
+// reproduces.  The control header is loaded and stored with 16-byte vector
+// accesses so the decision costs one memory round trip, not one per field.
+// Returns the next action (kActNone when the traversal is over).
+__device__ uint32_t decide_core(const DobfsParams& p) {
+  const unsigned long long now = globaltimer();
+  constexpr int            kV  = sizeof(CtrlHdr) / 16;
+  CtrlHdr                  c;
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(&p.ctrl->h);
+    uint4*       dst = reinterpret_cast<uint4*>(&c);
+#pragma unroll
+    for (int i = 0; i < kV; ++i) dst[i] = __ldcg(src + i);
+  }
   const uint64_t N    = p.n;
   uint32_t       next = kActNone;
   bool           done = false, queue_decision = false;
 
   switch (c.action) {
     case kActNone:  // first iteration: frontier = {root}
-      queue_decision = true;
+      queue_decision         = true;
+      p.ctrl->t_first_decide = now - c.t_start;
       break;
-    case kActTD: {
+    case kActTD:
+    case kActTDSmall: {
       const uint32_t nxt = c.cur ^ 1u;
-      const uint64_t nq  = qsum(c, nxt);
-      trace_add(c, 0, qsum(c, c.cur), nq);
+      const uint64_t nq  = frontier_size(c, nxt);
+      trace_add(p.ctrl, c, 0, frontier_size(c, c.cur), nq, now);
       c.td_steps++;
       c.reached += nq;
       c.scout_count = c.acc_scout;  // bfs.hpp:271
@@ -181,7 +578,7 @@ __global__ void k_decide(DobfsParams p) {
     }
     case kActBU: {
       const uint64_t awake = c.acc_awake;
-      trace_add(c, 1, c.old_awake, awake);
+      trace_add(p.ctrl, c, 1, c.old_awake, awake, now);
       c.bu_steps++;
       c.reached += awake;
       c.bm ^= 1u;  // C[bm] now holds this pull's discoveries (the new "front")
@@ -191,13 +588,14 @@ __global__ void k_decide(DobfsParams p) {
         c.awake_count = awake;
         c.acc_awake   = 0;
         c.bu_mode     = 1;
-        next          = kActBU;
+            next          = kActBU;
       } else if (awake == 0) {
         done = true;  // bfs.hpp:231-233
       } else {
         c.awake_count = awake;
-        for (int b = 0; b < kNumBins; ++b) c.qcount[c.cur][b] = 0;
-        next = kActB2Q;  // bfs.hpp:235-239
+        c.qpos[c.cur] = 0;
+        c.qbig[c.cur] = 0;
+        next          = kActB2Q;  // bfs.hpp:235-239
       }
       break;
     }
@@ -213,196 +611,238 @@ __global__ void k_decide(DobfsParams p) {
   }
 
   if (queue_decision) {
-    const uint64_t nq = qsum(c, c.cur);
+    const uint64_t nq = frontier_size(c, c.cur);
     if (!c.topdown_only && c.scout_count > c.edges_to_check / c.alpha) {  // bfs.hpp:186
       c.awake_count = nq;                                                // bfs.hpp:199-202
       c.old_awake   = nq;
       c.acc_awake   = 0;
       c.bu_mode     = 0;
       c.bm          = 1;  // the first pull writes C0
-      next          = kActBU;
+        next          = kActBU;
     } else {
       c.edges_to_check -= c.scout_count;  // bfs.hpp:244
       const uint32_t nxt = c.cur ^ 1u;
-      for (int b = 0; b < kNumBins; ++b) c.qcount[nxt][b] = 0;
+      c.qpos[nxt] = 0;
+      c.qbig[nxt] = 0;
       c.acc_scout = 0;
-      next        = kActTD;
+      // warp work units of the step: chunk entries + groups of 32 small vertices
+      const uint64_t units = (c.qpos[c.cur] >> 32) + ((c.qpos[c.cur] & 0xFFFFFFFFull) + 31) / 32;
+      next                 = units <= (uint64_t)kSmallBlocks * kWarps ? kActTDSmall : kActTD;
     }
   }
   if (!done && ++c.steps > c.max_steps) {
     c.status = NWG_ETIMEDOUT;  // loop bound; a BFS needs at most ~2n actions
   }
+  if (c.status == 0 && *(volatile int32_t*)&p.ctrl->err != 0) c.status = p.ctrl->err;
   if (c.status != 0) done = true;
-  c.action = done ? kActNone : next;
-  cudaGraphSetConditional(p.h_switch, done ? (unsigned)kActNone : next);
-  cudaGraphSetConditional(p.h_loop, done ? 0u : 1u);
-}
-
-// ---------------------------------------------------------------------------
-// Warp-aggregated append of discovered vertices into the degree-binned queue
-// `qi`: one atomicAdd per (warp, bin) instead of one per vertex.  All 32
-// lanes must call.
-__device__ __forceinline__ void append_binned(const DobfsParams& p, uint32_t qi, bool has, uint32_t v, int bin) {
-  Ctrl*          c    = p.ctrl;
-  const unsigned lane = threadIdx.x & 31;
+  c.action      = done ? kActNone : next;
+  c.pre_decided = 0;
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(&c);
+    uint4*       dst = reinterpret_cast<uint4*>(&p.ctrl->h);
 #pragma unroll
-  for (int b = 0; b < kNumBins; ++b) {
-    const unsigned m = __ballot_sync(kFullMask, has && bin == b);
-    if (m == 0) continue;
-    const int leader = __ffs(m) - 1;
-    uint32_t  base   = 0;
-    if ((int)lane == leader) base = atomicAdd(&c->qcount[qi][b], (uint32_t)__popc(m));
-    base = __shfl_sync(kFullMask, base, leader);
-    if (has && bin == b) {
-      const uint32_t pos = base + __popc(m & lanemask_lt());
-      if (pos < p.qcap[b]) {
-        p.q[qi][b][pos] = v;
-      } else {
-        c->status = NWG_EOVERFLOW;
-      }
-    }
+    for (int i = 0; i < kV; ++i) dst[i] = src[i];
   }
+  return c.action;
 }
 
-// One top-down edge test u -> v (bfs.hpp:280-289): claim v in V; the winner
-// writes parents[v] = u, adds out-degree(v) to scout and appends v.
-// All 32 lanes must call.
-__device__ __forceinline__ void td_visit(const DobfsParams& p, uint32_t* __restrict__ parents, uint32_t nxt,
-                                         bool valid, uint32_t u, uint32_t v, unsigned long long& scout) {
-  bool win = false;
-  if (valid) {
-    const uint32_t w   = v >> 5;
-    const uint32_t bit = 1u << (v & 31);
-    if (!(__ldcg(p.V + w) & bit)) {
-      const uint32_t old = atomicOr(p.V + w, bit);
-      win                = !(old & bit);
-    }
+// k_decide: the level loop's decision node.  When the previous action (the
+// persistent small-frontier kernel) already decided, it only applies that
+// decision to the graph's conditional handles.
+__global__ void k_decide(DobfsParams p) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  uint32_t next;
+  if (__ldcg(&p.ctrl->h.pre_decided)) {
+    next                  = __ldcg(&p.ctrl->h.action);
+    p.ctrl->h.pre_decided = 0;
+  } else {
+    next = decide_core(p);
   }
-  if (__ballot_sync(kFullMask, win) == 0) return;
-  int bin = 0;
-  if (win) {
-    parents[v]       = u;
-    const uint64_t d = p.off[v + 1] - p.off[v];
-    scout += d;
-    bin = degree_bin(d, p.th);
-  }
-  append_binned(p, nxt, win, v, bin);
-}
-
-// Expand out-edges [beg, end) of u with `nthr` cooperating threads (rank
-// `tr`); 128-bit non-coherent loads for the 16-byte-aligned body.  Trip
-// counts depend only on (beg, end, nthr), so every warp stays converged.
-__device__ __forceinline__ void expand_range(const DobfsParams& p, uint32_t* __restrict__ parents, uint32_t nxt,
-                                             uint32_t u, uint64_t beg, uint64_t end, uint32_t tr, uint32_t nthr,
-                                             unsigned long long& scout) {
-  const uint64_t a = min(end, (beg + 3) & ~(uint64_t)3);
-  for (uint64_t base = beg; base < a; base += nthr) {  // unaligned head (< 4 entries)
-    const uint64_t i     = base + tr;
-    const bool     valid = i < a;
-    td_visit(p, parents, nxt, valid, u, valid ? __ldg(p.col + i) : 0u, scout);
-  }
-  const uint64_t nvec = (end - a) >> 2;
-  const uint4*   col4 = reinterpret_cast<const uint4*>(p.col + a);
-  for (uint64_t base = 0; base < nvec; base += nthr) {
-    const uint64_t i     = base + tr;
-    const bool     valid = i < nvec;
-    uint4          x     = make_uint4(0, 0, 0, 0);
-    if (valid) x = __ldg(col4 + i);
-    td_visit(p, parents, nxt, valid, u, x.x, scout);
-    td_visit(p, parents, nxt, valid, u, x.y, scout);
-    td_visit(p, parents, nxt, valid, u, x.z, scout);
-    td_visit(p, parents, nxt, valid, u, x.w, scout);
-  }
-  const uint64_t t0 = a + (nvec << 2);
-  for (uint64_t base = t0; base < end; base += nthr) {  // tail (< 4 entries)
-    const uint64_t i     = base + tr;
-    const bool     valid = i < end;
-    td_visit(p, parents, nxt, valid, u, valid ? __ldg(p.col + i) : 0u, scout);
+  if (p.set_cond) {
+    cudaGraphSetConditional(p.h_switch, next);
+    cudaGraphSetConditional(p.h_loop, next == kActNone ? 0u : 1u);
   }
 }
 
 // ---------------------------------------------------------------------------
-// k_td: one top-down step (bfs.hpp:242-295) over the four degree bins.
-__global__ void __launch_bounds__(kThreads) k_td(DobfsParams p) {
-  Ctrl*           c       = p.ctrl;
-  const uint32_t  cur     = c->cur;
-  const uint32_t  nxt     = cur ^ 1u;
-  uint32_t* const parents = c->parents;
-  const uint32_t  nS = c->qcount[cur][kBinS], nM = c->qcount[cur][kBinM];
-  const uint32_t  nL = c->qcount[cur][kBinL], nH = c->qcount[cur][kBinH];
-  const unsigned  lane   = threadIdx.x & 31;
-  const uint64_t  wpb    = blockDim.x >> 5;
-  const uint64_t  gwarp  = blockIdx.x * wpb + (threadIdx.x >> 5);
-  const uint64_t  nwarps = gridDim.x * wpb;
-  unsigned long long scout = 0;
+// One top-down step (bfs.hpp:242-295) by blocks [0, nblocks): chunk entries
+// first (256-edge pieces of every vertex with out-degree >= warp_min, so
+// hubs spread over the grid), then the small-degree queue; both go through
+// gather_ranges, a group of entries per warp.  The group size of chunk
+// entries shrinks when there are few so every warp gets work.
+__device__ __forceinline__ void td_step(const DobfsParams& p, TdWarp* tws, uint32_t block, uint32_t nblocks) {
+  CtrlHdr*           c       = &p.ctrl->h;
+  const uint32_t     cur     = __ldcg(&c->cur);
+  const uint32_t     nxt     = cur ^ 1u;
+  uint32_t* const    parents = c->parents;
+  const uint64_t     qpos    = __ldcg(&c->qpos[cur]);
+  const uint64_t     nS      = min((uint64_t)(qpos & 0xFFFFFFFFull), p.qs_cap);
+  const uint64_t     nC      = min((uint64_t)(qpos >> 32), p.qc_cap);
+  TdWarp&            tw      = tws[threadIdx.x >> 5];
+  uint32_t           nbig    = 0;
+  const unsigned     lane    = threadIdx.x & 31;
+  const uint64_t     gwarp   = (uint64_t)block * kWarps + (threadIdx.x >> 5);
+  const uint64_t     nwarps  = (uint64_t)nblocks * kWarps;
+  uint32_t           wcnt    = 0;
+  unsigned long long scout   = 0;
 
-  // H: every CTA takes chunks of each huge vertex's edge list.
-  const uint64_t chunk = (uint64_t)blockDim.x * 16;
-  for (uint32_t i = 0; i < nH; ++i) {
-    const uint32_t u   = p.q[cur][kBinH][i];
-    const uint64_t beg = p.off[u], end = p.off[u + 1];
-    const uint64_t nch = (end - beg + chunk - 1) / chunk;
-    for (uint64_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
-      const uint64_t cb = beg + ch * chunk;
-      expand_range(p, parents, nxt, u, cb, min(end, cb + chunk), threadIdx.x, blockDim.x, scout);
+  uint64_t gsz = 1;  // chunk entries per warp group: at least ~4 groups per warp
+  while (gsz < 32 && nC > nwarps * gsz * 4) gsz <<= 1;
+  const uint64_t* qc = p.qc[cur];
+  for (uint64_t g0 = gwarp * gsz; g0 < nC; g0 += nwarps * gsz) {
+    const uint64_t i  = g0 + lane;
+    uint32_t       u  = 0;
+    uint64_t       lo = 0, hi = 0;
+    if (lane < gsz && i < nC) {
+      const uint64_t ent = __ldcg(qc + i);  // L2: written by other SMs earlier in a persistent launch
+      u                  = (uint32_t)(ent >> 32);
+      const uint64_t ob = p.off[u], oe = p.off[u + 1];
+      lo = ob + (ent & 0xFFFFFFFFull) * p.th.chunk;
+      hi = min(oe, lo + p.th.chunk);
     }
+    gather_ranges(p, parents, nxt, u, lo, hi, tw, wcnt, scout, nbig);
   }
-  // L: one CTA per vertex.
-  for (uint32_t i = blockIdx.x; i < nL; i += gridDim.x) {
-    const uint32_t u = p.q[cur][kBinL][i];
-    expand_range(p, parents, nxt, u, p.off[u], p.off[u + 1], threadIdx.x, blockDim.x, scout);
-  }
-  // M: one warp per vertex.
-  for (uint64_t i = gwarp; i < nM; i += nwarps) {
-    const uint32_t u = p.q[cur][kBinM][i];
-    expand_range(p, parents, nxt, u, p.off[u], p.off[u + 1], lane, 32, scout);
-  }
-  // S: 32 low-degree vertices per warp, their edge lists flattened by a warp
-  // scan and dealt out one edge per lane (scan-based gather).
+
+  const uint32_t* qs = p.qs[cur];
   for (uint64_t g0 = gwarp * 32; g0 < nS; g0 += nwarps * 32) {
-    const uint64_t qi   = g0 + lane;
-    const bool     have = qi < nS;
-    const uint32_t u    = have ? p.q[cur][kBinS][qi] : 0u;
-    const uint64_t beg  = have ? p.off[u] : 0;
-    const uint32_t deg  = have ? (uint32_t)(p.off[u + 1] - beg) : 0u;
-    uint32_t       incl = deg;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t t = __shfl_up_sync(kFullMask, incl, o);
-      if ((int)lane >= o) incl += t;
+    const uint64_t i  = g0 + lane;
+    uint32_t       u  = 0;
+    uint64_t       lo = 0, hi = 0;
+    if (i < nS) {
+      u  = __ldcg(qs + i);
+      lo = p.off[u];
+      hi = p.off[u + 1];
     }
-    const uint32_t total = __shfl_sync(kFullMask, incl, 31);
-    const uint32_t excl  = incl - deg;
-    for (uint32_t j = 0; j < total; j += 32) {
-      const uint32_t e     = j + lane;
-      const bool     valid = e < total;
-      int            lo    = 0;  // largest lane whose exclusive prefix <= e
-#pragma unroll
-      for (int s = 16; s >= 1; s >>= 1) {
-        const uint32_t ex = __shfl_sync(kFullMask, excl, lo + s);
-        if (ex <= e) lo += s;
-      }
-      const uint32_t ex_o  = __shfl_sync(kFullMask, excl, lo);
-      const uint64_t beg_o = __shfl_sync(kFullMask, beg, lo);
-      const uint32_t u_o   = __shfl_sync(kFullMask, u, lo);
-      const uint32_t v     = valid ? __ldg(p.col + beg_o + (e - ex_o)) : 0u;
-      td_visit(p, parents, nxt, valid, u_o, v, scout);
-    }
+    gather_ranges(p, parents, nxt, u, lo, hi, tw, wcnt, scout, nbig);
   }
+  flush_block(p, tws, wcnt, nxt, scout, nbig, true);
 
   const unsigned long long tot = block_sum(scout);
-  if (threadIdx.x == 0 && tot) atomicAdd(&c->acc_scout, tot);
+  __syncthreads();
+  const uint32_t nb = block_sum(nbig);
+  if (threadIdx.x == 0) {
+    if (tot) atomicAdd(&c->acc_scout, tot);
+    if (nb) atomicAdd(&c->qbig[nxt], nb);
+  }
+}
+
+// k_td: one top-down step over the whole grid.
+__global__ void __launch_bounds__(kThreads, 3) k_td(DobfsParams p) {
+  __shared__ TdWarp s_tw[kWarps];
+  td_step(p, s_tw, blockIdx.x, gridDim.x);
+}
+
+// Grid-wide barrier of a cooperative launch.  The wait is bounded: after
+// kBarrierSpins polls the block records NWG_ETIMEDOUT in ctrl->err and
+// returns false, and every later barrier returns false at once, so a
+// broken barrier can never hang the GPU.
+constexpr unsigned kBarrierSpins = 1u << 22;
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* a) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(a) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ bool grid_barrier(const DobfsParams& p, unsigned nblocks) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int      ok  = __ldcg(&p.ctrl->err) == 0;
+    GridBar* bar = &p.ctrl->bar;
+    if (ok) {
+      const unsigned g = ld_acquire(&bar->gen);
+      __threadfence();
+      if (atomicAdd(&bar->count, 1u) == nblocks - 1) {
+        atomicExch(&bar->count, 0u);
+        __threadfence();
+        atomicAdd(&bar->gen, 1u);
+      } else {
+        unsigned spins = 0;
+        while (ld_acquire(&bar->gen) == g) {
+          if (++spins > kBarrierSpins) {
+            atomicCAS(&p.ctrl->err, 0, NWG_ETIMEDOUT);
+            ok = 0;
+            break;
+          }
+          __nanosleep(32);
+        }
+      }
+      __threadfence();
+    }
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// k_td_loop: the small-frontier branch.  A persistent cooperative kernel of
+// kSmallBlocks blocks runs consecutive top-down steps, each followed by a
+// grid barrier and the decision (block 0), while the frontier stays small
+// and the direction stays top-down; it then leaves the next decision for
+// the graph's decide node (pre_decided).  Long, thin traversals (grids,
+// roads) thus pay a barrier per level instead of two kernel launches.
+__global__ void __launch_bounds__(kThreads) k_td_loop(DobfsParams p) {
+  __shared__ TdWarp   s_tw[kWarps];
+  __shared__ uint32_t s_next;
+  for (;;) {
+    td_step(p, s_tw, blockIdx.x, gridDim.x);
+    if (!grid_barrier(p, gridDim.x)) break;
+    if (blockIdx.x == 0 && threadIdx.x == 0) s_next = decide_core(p);
+    if (!grid_barrier(p, gridDim.x)) break;
+    if (threadIdx.x == 0) s_next = __ldcg(&p.ctrl->h.action);
+    __syncthreads();
+    if (s_next != kActTDSmall) break;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (__ldcg(&p.ctrl->err) != 0) {
+      // a barrier ran out: end the traversal with the error
+      p.ctrl->h.status = __ldcg(&p.ctrl->err);
+      p.ctrl->h.action = kActNone;
+    }
+    __threadfence();
+    p.ctrl->h.pre_decided = 1;
+  }
 }
 
 // ---------------------------------------------------------------------------
-// k_bu: one bottom-up pull (bfs.hpp:211-228).  A warp owns 32 vertices (one
-// bitmap word): it skips the word when none is a candidate, each candidate
-// lane probes its first in-edges, and the warp then scans the remaining
-// in-edges of unresolved lanes 32 at a time, stopping at the first hit.  The
-// first hit in row order becomes the parent, exactly as the reference's
-// sequential scan with break.
+// Candidate compaction shared by k_bu and k_b2q: lane `lane` holds bitmap
+// word `bits` of a 32-word tile; the set bits are written to `list` as local
+// vertex indices (word * 32 + bit).  Returns the count (warp-uniform).
+__device__ __forceinline__ uint32_t compact_tile(uint32_t bits, uint16_t* list) {
+  const unsigned lane  = threadIdx.x & 31;
+  const uint32_t cnt   = __popc(bits);
+  const uint32_t incl  = warp_incl_scan(cnt);
+  const uint32_t total = __shfl_sync(kFullMask, incl, 31);
+  uint32_t       pos   = incl - cnt;
+  while (bits) {
+    const int b = __ffs(bits) - 1;
+    bits &= bits - 1;
+    list[pos++] = (uint16_t)(lane * 32 + b);
+  }
+  __syncwarp();
+  return total;
+}
+
+// ---------------------------------------------------------------------------
+// k_bu: one bottom-up pull (bfs.hpp:211-228).
+//
+// Warps take tiles of kBuTileWords bitmap words (256 vertices), interleaved
+// over the grid (about seven tiles per warp at 2^24 vertices, so uneven tiles
+// average out).  A lane reads one word of
+// V, of the previous pull's C and of Z, folds C into V (the owner is the only
+// writer), and the tile's candidates (unvisited, with in-edges) are compacted
+// into a per-warp list in shared memory.  The
+// warp then takes 32 candidates at a time, one per lane, so 32 independent
+// in-edge scans are in flight per warp regardless of how sparse the
+// candidates are.  A lane scans its first kBuLane in-neighbours alone,
+// kBuProbe per round with independent loads; lanes still unresolved with
+// edges left are scanned by the whole warp, 32 in-edges per step.  The first hit in row order becomes the parent, exactly as the
+// reference's sequential scan with `break`.
 __global__ void __launch_bounds__(kThreads) k_bu(DobfsParams p) {
-  Ctrl*           c       = p.ctrl;
+  __shared__ uint16_t s_cand[kWarps][kBuTileWords * 32];
+  __shared__ uint32_t s_new[kWarps][kBuTileWords];
+  CtrlHdr*        c       = &p.ctrl->h;
   const uint32_t  mode    = c->bu_mode;
   const uint32_t  bm      = c->bm;
   uint32_t* const parents = c->parents;
@@ -410,41 +850,68 @@ __global__ void __launch_bounds__(kThreads) k_bu(DobfsParams p) {
   uint32_t*       Cw      = bm ? p.C0 : p.C1;  // this pull's discoveries
   const uint32_t* front   = mode ? Cf : p.V;
   const unsigned  lane    = threadIdx.x & 31;
-  const uint64_t  wpb     = blockDim.x >> 5;
-  const uint64_t  gwarp   = blockIdx.x * wpb + (threadIdx.x >> 5);
-  const uint64_t  nwarps  = gridDim.x * wpb;
+  const unsigned  wib     = threadIdx.x >> 5;
+  uint16_t* const cand    = s_cand[wib];
+  uint32_t* const fresh   = s_new[wib];
+  const uint64_t  ntiles  = (p.nwords + kBuTileWords - 1) / kBuTileWords;
   uint32_t        awake   = 0;
 
-  for (uint64_t w = gwarp; w < p.nwords; w += nwarps) {
-    const uint32_t vw = p.V[w];
-    const uint32_t fw = mode ? Cf[w] : 0u;
-    if (fw && lane == 0) p.V[w] = vw | fw;  // fold the previous pull into V
-    const uint32_t cand  = ~(vw | fw) & ~p.Z[w];
-    bool           found = false;
-    uint32_t       par   = 0;
-    if (cand) {
-      const uint64_t u    = w * 32 + lane;
-      const bool     mine = (cand >> lane) & 1u;
+  const uint64_t  gwarp   = (uint64_t)blockIdx.x * kWarps + wib;
+  const uint64_t  nwarps  = (uint64_t)gridDim.x * kWarps;
+  for (uint64_t t = gwarp; t < ntiles; t += nwarps) {
+    const uint64_t w  = t * kBuTileWords + lane;
+    const bool     wv = lane < kBuTileWords && w < p.nwords;
+    uint32_t       cm = 0;
+    if (wv) {
+      const uint32_t vw = p.V[w];
+      const uint32_t fw = mode ? Cf[w] : 0u;
+      if (fw) p.V[w] = vw | fw;  // fold the previous pull into V
+      cm = ~(vw | fw) & ~p.Z[w];
+    }
+    if (lane < kBuTileWords) fresh[lane] = 0;
+    const uint32_t total = compact_tile(cm, cand);
+
+    const uint64_t vbase = t * kBuTileWords * 32;
+    for (uint32_t j = 0; j < total; j += 32) {
+      const bool     mine = j + lane < total;
+      const uint32_t loc  = mine ? cand[j + lane] : 0u;
+      const uint64_t u    = vbase + loc;
       uint64_t       beg = 0, end = 0;
       if (mine) {
         beg = p.in_off[u];
         end = p.in_off[u + 1];
       }
-      const uint64_t lim = min(end, beg + kBuProbe);
-      uint64_t       e   = beg;
-      for (; e < lim; ++e) {
-        const uint32_t v = __ldg(p.in_col + e);
-        if ((__ldg(front + (v >> 5)) >> (v & 31)) & 1u) {
-          found = true;
-          par   = v;
-          break;
+      bool           found = false;
+      uint32_t       par   = 0;
+      uint64_t       e     = beg;
+      const uint64_t lim   = min(end, beg + kBuLane);
+      // each lane scans its own first kBuLane in-edges, kBuProbe per round
+      // (independent column and bitmap loads), until a hit
+      while (__any_sync(kFullMask, mine && !found && e < lim)) {
+        if (mine && !found && e < lim) {
+          uint32_t nb[kBuProbe];
+#pragma unroll
+          for (int k = 0; k < kBuProbe; ++k) nb[k] = (e + k < lim) ? __ldg(p.in_col + e + k) : kNull;
+          uint32_t hit = 0;
+#pragma unroll
+          for (int k = 0; k < kBuProbe; ++k)
+            if (nb[k] != kNull && ((__ldg(front + (nb[k] >> 5)) >> (nb[k] & 31)) & 1u)) hit |= 1u << k;
+          if (hit) {
+            const int k = __ffs(hit) - 1;
+#pragma unroll
+            for (int q = 0; q < kBuProbe; ++q)
+              if (q == k) par = nb[q];
+            found = true;
+          }
+          e = min(lim, e + kBuProbe);
         }
       }
-      unsigned pend = __ballot_sync(kFullMask, mine && !found && e < end);
+      const uint64_t rest = e;  // long lists: the whole warp scans the rest
+      unsigned       pend = __ballot_sync(kFullMask, mine && !found && rest < end);
       while (pend) {
         const int leader = __ffs(pend) - 1;
         pend &= pend - 1;
-        const uint64_t b  = __shfl_sync(kFullMask, e, leader);
+        const uint64_t b  = __shfl_sync(kFullMask, rest, leader);
         const uint64_t en = __shfl_sync(kFullMask, end, leader);
         for (uint64_t base = b; base < en; base += 32) {
           const uint64_t i = base + lane;
@@ -465,46 +932,59 @@ __global__ void __launch_bounds__(kThreads) k_bu(DobfsParams p) {
           }
         }
       }
+      if (found) {
+        parents[u] = par;
+        atomicOr(&fresh[loc >> 5], 1u << (loc & 31));
+      }
     }
-    const unsigned nb = __ballot_sync(kFullMask, found);
-    if (found) parents[w * 32 + lane] = par;
-    if (lane == 0) {
-      Cw[w] = nb;
-      awake += __popc(nb);
+    __syncwarp();
+    if (wv) {
+      const uint32_t nw = fresh[lane];
+      Cw[w]             = nw;
+      awake += __popc(nw);
     }
+    __syncwarp();
   }
   const uint32_t tot = block_sum(awake);
   if (threadIdx.x == 0 && tot) atomicAdd(&c->acc_awake, (unsigned long long)tot);
 }
 
 // ---------------------------------------------------------------------------
-// k_b2q: bitmap -> binned queue (bfs.hpp:235-239) from C[bm], folding C[bm]
-// into V on the way.  Each warp reads 32 words and expands the non-zero ones
-// one at a time, one bit per lane.
+// k_b2q: bitmap -> queue (bfs.hpp:235-239) from C[bm], folding C[bm] into V
+// on the way.  Each warp compacts tiles of 32 words into its vertex buffer;
+// full buffers are appended per warp, the rest once per block at the end.
 __global__ void __launch_bounds__(kThreads) k_b2q(DobfsParams p) {
-  Ctrl*           c      = p.ctrl;
-  const uint32_t* Cs     = c->bm ? p.C1 : p.C0;
-  const uint32_t  qi     = c->cur;
-  const unsigned  lane   = threadIdx.x & 31;
-  const uint64_t  wpb    = blockDim.x >> 5;
-  const uint64_t  gwarp  = blockIdx.x * wpb + (threadIdx.x >> 5);
-  const uint64_t  nwarps = gridDim.x * wpb;
-  for (uint64_t w0 = gwarp * 32; w0 < p.nwords; w0 += nwarps * 32) {
-    const uint64_t w = w0 + lane;
+  __shared__ uint16_t s_list[kWarps][kTileWords * 32];
+  __shared__ TdWarp   s_tw[kWarps];
+  CtrlHdr*           c      = &p.ctrl->h;
+  const uint32_t*    Cs     = c->bm ? p.C1 : p.C0;
+  const uint32_t     qi     = c->cur;
+  const unsigned     lane   = threadIdx.x & 31;
+  const unsigned     wib    = threadIdx.x >> 5;
+  const uint64_t     gwarp  = (uint64_t)blockIdx.x * kWarps + wib;
+  const uint64_t     nwarps = (uint64_t)gridDim.x * kWarps;
+  const uint64_t     ntiles = (p.nwords + kTileWords - 1) / kTileWords;
+  uint16_t* const    list   = s_list[wib];
+  TdWarp&            tw     = s_tw[wib];
+  uint32_t           wcnt   = 0, nbig = 0;
+  unsigned long long scout  = 0;
+  for (uint64_t t = gwarp; t < ntiles; t += nwarps) {
+    const uint64_t w = t * kTileWords + lane;
     const uint32_t x = (w < p.nwords) ? Cs[w] : 0u;
     if (x) p.V[w] |= x;
-    unsigned nz = __ballot_sync(kFullMask, x != 0);
-    while (nz) {
-      const int src = __ffs(nz) - 1;
-      nz &= nz - 1;
-      const uint32_t word = __shfl_sync(kFullMask, x, src);
-      const uint32_t v    = (uint32_t)((w0 + src) * 32 + lane);
-      const bool     has  = (word >> lane) & 1u;
-      int            bin  = 0;
-      if (has) bin = degree_bin(p.off[v + 1] - p.off[v], p.th);
-      append_binned(p, qi, has, v, bin);
+    const uint32_t total = compact_tile(x, list);
+    const uint64_t vbase = t * kTileWords * 32;
+    for (uint32_t j = 0; j < total; j += 32) {
+      const uint32_t k = min(32u, total - j);  // warp-uniform
+      if (wcnt + k > kWinBuf) flush_winners(p, tw, wcnt, qi, scout, nbig);
+      if (lane < k) tw.win[wcnt + lane] = (uint32_t)(vbase + list[j + lane]);
+      wcnt += k;
     }
+    __syncwarp();
   }
+  flush_block(p, s_tw, wcnt, qi, scout, nbig, false);
+  const uint32_t nb = block_sum(nbig);
+  if (threadIdx.x == 0 && nb) atomicAdd(&c->qbig[qi], nb);
 }
 
 // In-degree-zero bitmap; bits past n are set so they are never candidates.
@@ -552,6 +1032,7 @@ int build_exec(Workspace* ws) {
   GraphDev*   g = ws->g;
   cudaGraph_t graph;
   NWG_CUDA_TRY(cudaGraphCreate(&graph, 0));
+  ws->template_graph = graph;
   cudaGraphConditionalHandle h_loop, h_switch;
   NWG_CUDA_TRY(cudaGraphConditionalHandleCreate(&h_loop, graph, 1, cudaGraphCondAssignDefault));
 
@@ -580,6 +1061,7 @@ int build_exec(Workspace* ws) {
   NWG_CUDA_TRY(cudaGraphConditionalHandleCreate(&h_switch, body, kActNone, cudaGraphCondAssignDefault));
   P.h_loop   = h_loop;
   P.h_switch = h_switch;
+  P.set_cond = 1;
 
   void*                decide_args[] = {&P};
   cudaKernelNodeParams dp            = {};
@@ -598,28 +1080,28 @@ int build_exec(Workspace* ws) {
   cudaGraphNode_t switch_node;
   NWG_CUDA_TRY(cudaGraphAddNode(&switch_node, body, &decide_node, 1, &sp));
 
-  void* (kernels[kNumActions]) = {(void*)k_td, (void*)k_bu, (void*)k_b2q};
-  const int per_sm[kNumActions] = {8, 8, 8};
+  void*     kernels[kNumActions] = {(void*)k_td, (void*)k_bu, (void*)k_b2q, (void*)k_td_loop};
+  const int grids[kNumActions]   = {grid_for(g, kTdPerSm), grid_for(g, 8), grid_for(g, 8), kSmallBlocks};
   for (int a = 0; a < kNumActions; ++a) {
     void*                args[] = {&P};
     cudaKernelNodeParams ap     = {};
     ap.func                     = kernels[a];
-    ap.gridDim                  = dim3(grid_for(g, per_sm[a]));
+    ap.gridDim                  = dim3(grids[a]);
     ap.blockDim                 = dim3(kThreads);
     ap.kernelParams             = args;
     cudaGraphNode_t n;
     NWG_CUDA_TRY(cudaGraphAddKernelNode(&n, sp.conditional.phGraph_out[a], nullptr, 0, &ap));
+    if (a == kActTDSmall) {  // grid barriers need every block resident: cooperative launch
+      cudaLaunchAttributeValue v = {};
+      v.cooperative              = 1;
+      NWG_CUDA_TRY(cudaGraphKernelNodeSetAttribute(n, cudaLaunchAttributeCooperative, &v));
+    }
   }
 
   cudaGraphExec_t exec;
-  cudaError_t     e = cudaGraphInstantiate(&exec, graph, 0);
-  if (e != cudaSuccess) {
-    cudaGraphDestroy(graph);
-    return cuda_error(e, "cudaGraphInstantiate(level loop)");
-  }
+  NWG_CUDA_TRY(cudaGraphInstantiate(&exec, graph, 0));
   ws->exec[0]      = exec;
   ws->init_node[0] = init_node;
-  ws->template_graph = graph;
   return NWG_OK;
 }
 
@@ -631,20 +1113,20 @@ int ws_init(GraphDev* g, Workspace* ws) {
   const uint64_t n      = g->n;
   const uint32_t nwords = (uint32_t)((n + 31) / 32);
   const uint64_t m      = g->m;
-  uint64_t       cap[kNumBins];
-  cap[kBinS] = std::max<uint64_t>(n, 1);
-  cap[kBinM] = std::max<uint64_t>(1, std::min<uint64_t>(n, m / g->th.warp_min + 1));
-  cap[kBinL] = std::max<uint64_t>(1, std::min<uint64_t>(n, m / g->th.cta_min + 1));
-  cap[kBinH] = std::max<uint64_t>(1, std::min<uint64_t>(n, m / g->th.grid_min + 1));
-  uint64_t qtot = 0;
-  for (int b = 0; b < kNumBins; ++b) qtot += cap[b];
+  // A vertex enters a queue at most once per level: n small entries.  The
+  // chunked vertices have out-degree >= warp_min, so there are at most
+  // m / warp_min of them, with at most m / chunk + that many chunk entries.
+  const uint64_t qs_cap = std::max<uint64_t>(n, 1);
+  const uint64_t big    = std::min<uint64_t>(n, m / g->th.warp_min);
+  const uint64_t qc_cap = std::max<uint64_t>(1, m / g->th.chunk + big + 1);
 
   NWG_CUDA_TRY(cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking));
   NWG_CUDA_TRY(cudaEventCreate(&ws->ev0));
   NWG_CUDA_TRY(cudaEventCreate(&ws->ev1));
   if (cudaMalloc(&ws->parents, std::max<uint64_t>(n, 4) * sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(&ws->V, 3ull * std::max<uint32_t>(nwords, 1) * sizeof(uint32_t)) != cudaSuccess ||
-      cudaMalloc(&ws->qbuf, 2ull * qtot * sizeof(uint32_t)) != cudaSuccess ||
+      cudaMalloc(&ws->qbuf, 2ull * qs_cap * sizeof(uint32_t)) != cudaSuccess ||
+      cudaMalloc(&ws->cbuf, 2ull * qc_cap * sizeof(uint64_t)) != cudaSuccess ||
       cudaMalloc(&ws->ctrl, sizeof(Ctrl)) != cudaSuccess) {
     cudaGetLastError();
     return set_error(NWG_ENOMEM, "workspace allocation failed (n=" + std::to_string(n) + ")");
@@ -664,15 +1146,14 @@ int ws_init(GraphDev* g, Workspace* ws) {
   P.C0           = ws->V + std::max<uint32_t>(nwords, 1);
   P.C1           = ws->V + 2ull * std::max<uint32_t>(nwords, 1);
   P.Z            = g->Z;
-  uint32_t* qp   = ws->qbuf;
-  for (int q = 0; q < 2; ++q)
-    for (int b = 0; b < kNumBins; ++b) {
-      P.q[q][b] = qp;
-      qp += cap[b];
-    }
-  for (int b = 0; b < kNumBins; ++b) P.qcap[b] = (uint32_t)std::min<uint64_t>(cap[b], 0xFFFFFFFFull);
-  P.th   = g->th;
-  P.ctrl = ws->ctrl;
+  P.qs[0]        = ws->qbuf;
+  P.qs[1]        = ws->qbuf + qs_cap;
+  P.qc[0]        = ws->cbuf;
+  P.qc[1]        = ws->cbuf + qc_cap;
+  P.qs_cap       = qs_cap;
+  P.qc_cap       = qc_cap;
+  P.th           = g->th;
+  P.ctrl         = ws->ctrl;
   return build_exec(ws);
 }
 
@@ -690,6 +1171,7 @@ void ws_free(Workspace* ws) {
   cudaFree(ws->parents);
   cudaFree(ws->V);
   cudaFree(ws->qbuf);
+  cudaFree(ws->cbuf);
   cudaFree(ws->ctrl);
   if (ws->ctrl_host) cudaFreeHost(ws->ctrl_host);
   cudaSetDevice(prev);
@@ -702,7 +1184,7 @@ int ws_launch(Workspace* ws, uint32_t root, int alpha, int beta, uint32_t* paren
   if (root >= g->n) return set_error(NWG_EINVAL, "root " + std::to_string(root) + " >= n " + std::to_string(g->n));
   if (alpha <= 0 || beta <= 0) return set_error(NWG_EINVAL, "alpha and beta must be positive");
   uint32_t  r = root, a = (uint32_t)alpha, b = (uint32_t)beta, td = topdown_only ? 1u : 0u;
-  uint32_t* par = parents ? parents : ws->parents;
+  uint32_t* par    = parents ? parents : ws->parents;
   void*     args[] = {&ws->params, &r, &a, &b, &par, &td};
   cudaKernelNodeParams kp = {};
   kp.func                 = (void*)k_init;
@@ -715,20 +1197,56 @@ int ws_launch(Workspace* ws, uint32_t root, int alpha, int beta, uint32_t* paren
   return NWG_OK;
 }
 
+int ws_launch_stepped(Workspace* ws, uint32_t root, int alpha, int beta, uint32_t* parents, cudaStream_t stream) {
+  GraphDev* g = ws->g;
+  if (root >= g->n) return set_error(NWG_EINVAL, "root " + std::to_string(root) + " >= n " + std::to_string(g->n));
+  if (alpha <= 0 || beta <= 0) return set_error(NWG_EINVAL, "alpha and beta must be positive");
+  DobfsParams P = ws->params;
+  P.set_cond    = 0;
+  uint32_t* par = parents ? parents : ws->parents;
+  k_init<<<grid_for(g, 8), kThreads, 0, stream>>>(P, root, (uint32_t)alpha, (uint32_t)beta, par, 0u);
+  NWG_CUDA_TRY(cudaGetLastError());
+  const uint64_t cap = 2 * g->n + 64;
+  for (uint64_t step = 0; step <= cap; ++step) {
+    k_decide<<<1, 32, 0, stream>>>(P);
+    NWG_CUDA_TRY(cudaGetLastError());
+    uint32_t action = kActNone;
+    NWG_CUDA_TRY(cudaMemcpyAsync(&action, &ws->ctrl->h.action, sizeof(action), cudaMemcpyDeviceToHost, stream));
+    NWG_CUDA_TRY(cudaStreamSynchronize(stream));
+    if (action == kActTD) {
+      k_td<<<grid_for(g, kTdPerSm), kThreads, 0, stream>>>(P);
+    } else if (action == kActTDSmall) {
+      void* args[] = {&P};
+      NWG_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_td_loop, dim3(kSmallBlocks), dim3(kThreads), args, 0, stream));
+    } else if (action == kActBU) {
+      k_bu<<<grid_for(g, 8), kThreads, 0, stream>>>(P);
+    } else if (action == kActB2Q) {
+      k_b2q<<<grid_for(g, 8), kThreads, 0, stream>>>(P);
+    } else {
+      break;
+    }
+    NWG_CUDA_TRY(cudaGetLastError());
+  }
+  ws->ran = true;
+  return NWG_OK;
+}
+
 void fill_stats(const Ctrl& c, nwg_bfs_stats* s) {
-  s->status    = c.status;
-  s->steps     = c.steps;
-  s->levels    = c.levels;
-  s->td_steps  = c.td_steps;
-  s->bu_steps  = c.bu_steps;
-  s->b2q_steps = c.b2q_steps;
-  s->reached   = c.reached;
-  s->trace_len = std::min<uint32_t>(c.trace_len, NWG_TRACE_CAP);
+  s->status    = c.h.status ? c.h.status : c.err;
+  s->steps     = c.h.steps;
+  s->levels    = c.h.levels;
+  s->td_steps  = c.h.td_steps;
+  s->bu_steps  = c.h.bu_steps;
+  s->b2q_steps = c.h.b2q_steps;
+  s->reached   = c.h.reached;
+  s->trace_len = std::min<uint32_t>(c.h.trace_len, NWG_TRACE_CAP);
   for (uint32_t i = 0; i < s->trace_len; ++i) {
     s->trace_dir[i]      = c.trace_dir[i];
     s->trace_frontier[i] = c.trace_frontier[i];
     s->trace_found[i]    = c.trace_found[i];
+    s->trace_end_ns[i]   = c.trace_end_ns[i];
   }
+  s->first_decide_ns = c.t_first_decide;
 }
 
 int build_zero_indegree(GraphDev* g, cudaStream_t stream) {

@@ -148,12 +148,6 @@ __global__ void k_gather_deg(const uint64_t* __restrict__ off, const uint32_t* _
   if (i < count) out[i] = off[ids[i] + 1] - off[ids[i]];
 }
 
-int bits_for(uint64_t n) {
-  int b = 1;
-  while (b < 32 && (1ull << b) < n) ++b;
-  return b;
-}
-
 // keys[0, 2*count) -> sorted unique CSR in g (allocates g->off, g->col).
 int build_csr(uint64_t* keys, uint64_t nkeys, uint64_t n, GraphDev* g) {
   uint64_t* alt = nullptr;

@@ -16,27 +16,37 @@ namespace nwg {
 constexpr uint32_t kNull     = 0xFFFFFFFFu;
 constexpr unsigned kFullMask = 0xFFFFFFFFu;
 
-// Degree bins of the frontier queue: a vertex is expanded by a warp-shared
-// gather (S), one warp (M), one CTA (L) or the whole grid (H).
-enum Bin : int { kBinS = 0, kBinM = 1, kBinL = 2, kBinH = 3, kNumBins = 4 };
+// Frontier queues.  A vertex whose out-degree is below `warp_min` goes to
+// the small queue (ids; a warp expands 32 of them at once through a
+// scan-based gather); any other vertex is split into chunks of `chunk`
+// out-edges, one queue entry (vertex << 32 | chunk index) per chunk, and a
+// warp expands one chunk at a time.  Hubs are thus spread over the whole
+// grid instead of occupying one warp or CTA.
+// Queue fill level of buffer q: qpos[q] packs the small-queue entry count
+// (low 32 bits) and the chunk-queue entry count (high 32 bits) so one 64-bit
+// atomicAdd reserves space in both; qbig[q] counts the chunked vertices.
 
 // Actions of the device level loop (the switch node's branches).
-enum Action : uint32_t { kActTD = 0, kActBU = 1, kActB2Q = 2, kActNone = 3, kNumActions = 3 };
-
-struct Thresholds {
-  uint32_t warp_min;  // degree >= warp_min -> bin M
-  uint32_t cta_min;   // degree >= cta_min  -> bin L
-  uint32_t grid_min;  // degree >= grid_min -> bin H
+enum Action : uint32_t {
+  kActTD      = 0,  // top-down step, full grid
+  kActBU      = 1,  // bottom-up pull
+  kActB2Q     = 2,  // bitmap -> queue
+  kActTDSmall = 3,  // top-down step on a small frontier, small grid
+  kActNone    = 4,
+  kNumActions = 4
 };
 
-__host__ __device__ inline int degree_bin(uint64_t deg, const Thresholds& t) {
-  return deg >= t.grid_min ? kBinH : deg >= t.cta_min ? kBinL : deg >= t.warp_min ? kBinM : kBinS;
-}
+struct Thresholds {
+  uint32_t warp_min;     // out-degree >= warp_min -> chunked
+  uint32_t chunk;        // out-edges per chunk entry (a power of two)
+  uint32_t chunk_shift;  // log2(chunk)
+};
 
 // Device control block of one traversal.  Written by the init kernel, then
 // advanced by the decide kernel between actions; action kernels only add to
-// the accumulators and queue counters.
-struct Ctrl {
+// the accumulators and queue counters.  The header is read and written by
+// the decide kernel with 16-byte vector accesses (one memory round trip).
+struct alignas(16) CtrlHdr {
   uint32_t* parents;  // output array of this traversal
   uint32_t  root;
   uint32_t  alpha;
@@ -51,7 +61,8 @@ struct Ctrl {
   unsigned long long acc_scout;  // += out-degree of every vertex a top-down step discovers
   unsigned long long acc_awake;  // += vertices a bottom-up pull discovers
 
-  uint32_t qcount[2][kNumBins];  // entries per bin of queue buffer 0/1
+  unsigned long long qpos[2];    // [buffer] small entries | chunk entries << 32
+  uint32_t           qbig[2];    // [buffer] vertices in the chunk queue
   uint32_t cur;                  // queue buffer holding the frontier
   uint32_t bm;                   // bottom-up: index of the bitmap holding the latest pull's discoveries
   uint32_t bu_mode;              // 0: first pull of a phase (front = visited), 1: later pull (front = C[bm])
@@ -59,12 +70,28 @@ struct Ctrl {
 
   uint32_t steps, levels, td_steps, bu_steps, b2q_steps;
   int32_t  status;
+  uint32_t pre_decided;  // the previous action kernel already made the next decision
   unsigned long long reached;
+  unsigned long long t_start;  // %globaltimer at init (ns)
   uint32_t trace_len;
   uint32_t max_steps;
+};
+
+// Grid barrier of the persistent small-frontier kernel.
+struct GridBar {
+  alignas(128) unsigned int count;  // arrivals (own 128-byte line)
+  alignas(128) unsigned int gen;    // generation, polled with acquire loads (own line)
+};
+
+struct Ctrl {
+  CtrlHdr            h;
+  GridBar            bar;
+  int32_t            err;  // set with atomics by a device wait that ran out (never overwritten by the header copy)
   uint8_t            trace_dir[NWG_TRACE_CAP];
   unsigned long long trace_frontier[NWG_TRACE_CAP];
   unsigned long long trace_found[NWG_TRACE_CAP];
+  unsigned long long trace_end_ns[NWG_TRACE_CAP];  // %globaltimer - t_start when the step's result was consumed
+  unsigned long long t_first_decide;
 };
 
 // Static parameters of the level-loop kernels (baked into the CUDA graph).
@@ -80,12 +107,15 @@ struct DobfsParams {
   uint32_t*       C0;      // bottom-up discovery bitmaps [nwords] x 2
   uint32_t*       C1;
   const uint32_t* Z;       // in-degree-zero bitmap [nwords] (never discoverable bottom-up)
-  uint32_t*       q[2][kNumBins];
-  uint32_t        qcap[kNumBins];
+  uint32_t*       qs[2];  // small-degree vertex queues
+  uint64_t*       qc[2];  // chunk queues
+  uint64_t        qs_cap;
+  uint64_t        qc_cap;
   Thresholds      th;
   Ctrl*           ctrl;
   cudaGraphConditionalHandle h_loop;
   cudaGraphConditionalHandle h_switch;
+  uint32_t                   set_cond;  // 0 when the kernels are launched one by one from the host
 };
 
 struct GraphDev;
@@ -96,7 +126,8 @@ struct Workspace {
   int             device = 0;
   uint32_t*       parents = nullptr;  // default output
   uint32_t*       V = nullptr;        // V, C0, C1 in one allocation
-  uint32_t*       qbuf = nullptr;     // both queue buffers, all bins
+  uint32_t*       qbuf = nullptr;     // both small queues
+  uint64_t*       cbuf = nullptr;     // both chunk queues
   Ctrl*           ctrl = nullptr;     // device
   Ctrl*           ctrl_host = nullptr;  // pinned mirror for stats
   cudaStream_t    stream = nullptr;   // owned stream for the synchronous API
@@ -119,7 +150,7 @@ struct GraphDev {
   uint32_t* Z = nullptr;  // in-degree-zero bitmap
   bool      owns_out = false, owns_in = false, symmetric = true;
   int       sm_count = 148;
-  Thresholds th{32, 1024, 32768};
+  Thresholds th{32, 256, 8};
   std::mutex              mu;
   Workspace*              default_ws = nullptr;
   std::vector<Workspace*> workspaces;
@@ -139,6 +170,7 @@ int  ws_init(GraphDev* g, Workspace* ws);
 void ws_free(Workspace* ws);
 int  ws_launch(Workspace* ws, uint32_t root, int alpha, int beta, uint32_t* parents, cudaStream_t stream,
                bool topdown_only);
+int  ws_launch_stepped(Workspace* ws, uint32_t root, int alpha, int beta, uint32_t* parents, cudaStream_t stream);
 void fill_stats(const Ctrl& c, nwg_bfs_stats* s);
 int  build_zero_indegree(GraphDev* g, cudaStream_t stream);
 int  component_edges(GraphDev* g, const uint32_t* parents, uint64_t* edges, uint64_t* vertices);

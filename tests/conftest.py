@@ -61,8 +61,11 @@ def golden():
 @pytest.fixture(scope="session")
 def nwg():
     """The CUDA library; built in-tree first if it is missing (nvcc only)."""
-    from nwgr_b200 import build as B
+    import importlib.util
 
+    spec = importlib.util.spec_from_file_location("nwgr_b200_build", os.path.join(ROOT, "nwgr_b200", "build.py"))
+    B = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(B)
     B.build()
     import nwgr_b200
 
