@@ -139,6 +139,23 @@ int nwg_component_edges(nwg_graph g, const uint32_t* parents_dev, uint64_t* edge
  * host arrays of the sizes nwg_graph_info reports; any pointer may be NULL. */
 int nwg_graph_copy_csr(nwg_graph g, uint64_t* out_off, uint32_t* out_col, uint64_t* in_off, uint32_t* in_col);
 
+/* Direction-optimizing BFS that allocates no device memory.  No counterpart
+ * in the reference: NWGraph's bfs allocates its state per call.  For callers
+ * that may not call cudaMalloc/cudaFree (both synchronise the device; latency-
+ * bound services and processes whose device memory belongs to their own
+ * allocator forbid them).  The caller passes device arrays: uint64 offsets
+ * (n + 1), uint32 columns (16-byte aligned), optional in-CSR (NULL = the
+ * out-CSR, symmetric), and parents_dev (n entries).  All scratch lives in a
+ * static device array of fixed size: n <= 2^20 and m <= 2^24 (larger graphs
+ * return NWG_EINVAL before any launch).  Calls share that array: calls whose
+ * GPU work overlaps race, so serialise them.  The first call on a device
+ * looks the array's address up; make it before any stream capture.  The
+ * level loop is driven from the host (a small read-back per step) on
+ * `stream` (a cudaStream_t, NULL = legacy default stream); the call returns
+ * when the traversal is complete. */
+int nwg_bfs_noalloc(const uint64_t* out_off, const uint32_t* out_col, const uint64_t* in_off, const uint32_t* in_col,
+                    uint64_t n, uint32_t root, int alpha, int beta, uint32_t* parents_dev, void* stream);
+
 /* Seeded synthetic graph generators on the device (no reference
  * counterpart: NWGraph ships no RMAT/uniform/grid generator).  Each builds a
  * symmetrized, self-loop-free, deduplicated CSR with sorted rows directly in

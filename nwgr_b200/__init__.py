@@ -38,7 +38,7 @@ EXPORTED = (
     "nwg_version", "nwg_last_error", "nwg_graph_register", "nwg_graph_register_u32off", "nwg_graph_release",
     "nwg_graph_info", "nwg_bfs", "nwg_ws_create", "nwg_ws_destroy", "nwg_bfs_async", "nwg_ws_stats",
     "nwg_bfs_topdown", "nwg_bfs_stepped", "nwg_component_edges", "nwg_graph_copy_csr", "nwg_gen_rmat", "nwg_gen_uniform",
-    "nwg_gen_grid", "nwg_pick_roots",
+    "nwg_gen_grid", "nwg_pick_roots", "nwg_bfs_noalloc",
 )
 
 
@@ -100,6 +100,7 @@ def _load():
         "nwg_gen_uniform": (_int, [_u64, _u32, _u64, C.POINTER(_vp)]),
         "nwg_gen_grid": (_int, [_u32, _u32, _u32, _u64, C.POINTER(_vp)]),
         "nwg_pick_roots": (_int, [_vp, _u64, _u32, _vp]),
+        "nwg_bfs_noalloc": (_int, [_vp, _vp, _vp, _vp, _u64, _u32, _int, _int, _vp, _vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -290,6 +291,16 @@ def bfs_stepped(g: Graph, root: int, parents_dev=None, alpha: int = 15, beta: in
     s = Stats()
     check(lib.nwg_bfs_stepped(g.h, int(root), alpha, beta, _ptr(parents_dev), C.byref(s)))
     return s
+
+
+def bfs_noalloc(out_off_dev, out_col_dev, n: int, root: int, parents_dev, in_off_dev=None, in_col_dev=None,
+                alpha: int = 15, beta: int = 18, stream=None) -> None:
+    """nwg_bfs_noalloc: the traversal without any device allocation, for
+    callers that may not call cudaMalloc.  All arrays are the caller's device
+    memory (torch tensors or integer pointers); limits n <= 2^20, m <= 2^24.
+    Calls share one static scratch array: do not overlap them on the GPU."""
+    check(lib.nwg_bfs_noalloc(_ptr(out_off_dev), _ptr(out_col_dev), _ptr(in_off_dev), _ptr(in_col_dev), int(n),
+                              int(root), alpha, beta, _ptr(parents_dev), _ptr(stream)))
 
 
 def bfs_serial(graph: Graph, root: int, stats: bool = False):

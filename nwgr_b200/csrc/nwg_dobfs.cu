@@ -1197,37 +1197,56 @@ int ws_launch(Workspace* ws, uint32_t root, int alpha, int beta, uint32_t* paren
   return NWG_OK;
 }
 
-int ws_launch_stepped(Workspace* ws, uint32_t root, int alpha, int beta, uint32_t* parents, cudaStream_t stream) {
-  GraphDev* g = ws->g;
-  if (root >= g->n) return set_error(NWG_EINVAL, "root " + std::to_string(root) + " >= n " + std::to_string(g->n));
-  if (alpha <= 0 || beta <= 0) return set_error(NWG_EINVAL, "alpha and beta must be positive");
-  DobfsParams P = ws->params;
+// The level loop driven from the host: the kernels of the CUDA graph
+// launched one at a time on `stream`, the decision read back after every
+// step into host stack memory.  Allocates nothing.
+int run_stepped(const DobfsParams& params, int sm_count, uint32_t root, int alpha, int beta, uint32_t* parents,
+                cudaStream_t stream) {
+  DobfsParams P = params;
   P.set_cond    = 0;
-  uint32_t* par = parents ? parents : ws->parents;
-  k_init<<<grid_for(g, 8), kThreads, 0, stream>>>(P, root, (uint32_t)alpha, (uint32_t)beta, par, 0u);
+  const int big = std::max(1, sm_count * 8);
+  const int td  = std::max(1, sm_count * kTdPerSm);
+  k_init<<<big, kThreads, 0, stream>>>(P, root, (uint32_t)alpha, (uint32_t)beta, parents, 0u);
   NWG_CUDA_TRY(cudaGetLastError());
-  const uint64_t cap = 2 * g->n + 64;
+  const uint64_t cap = 2 * P.n + 64;
   for (uint64_t step = 0; step <= cap; ++step) {
     k_decide<<<1, 32, 0, stream>>>(P);
     NWG_CUDA_TRY(cudaGetLastError());
     uint32_t action = kActNone;
-    NWG_CUDA_TRY(cudaMemcpyAsync(&action, &ws->ctrl->h.action, sizeof(action), cudaMemcpyDeviceToHost, stream));
+    NWG_CUDA_TRY(cudaMemcpyAsync(&action, &P.ctrl->h.action, sizeof(action), cudaMemcpyDeviceToHost, stream));
     NWG_CUDA_TRY(cudaStreamSynchronize(stream));
     if (action == kActTD) {
-      k_td<<<grid_for(g, kTdPerSm), kThreads, 0, stream>>>(P);
+      k_td<<<td, kThreads, 0, stream>>>(P);
     } else if (action == kActTDSmall) {
       void* args[] = {&P};
       NWG_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_td_loop, dim3(kSmallBlocks), dim3(kThreads), args, 0, stream));
     } else if (action == kActBU) {
-      k_bu<<<grid_for(g, 8), kThreads, 0, stream>>>(P);
+      k_bu<<<big, kThreads, 0, stream>>>(P);
     } else if (action == kActB2Q) {
-      k_b2q<<<grid_for(g, 8), kThreads, 0, stream>>>(P);
+      k_b2q<<<big, kThreads, 0, stream>>>(P);
     } else {
       break;
     }
     NWG_CUDA_TRY(cudaGetLastError());
   }
-  ws->ran = true;
+  return NWG_OK;
+}
+
+int ws_launch_stepped(Workspace* ws, uint32_t root, int alpha, int beta, uint32_t* parents, cudaStream_t stream) {
+  GraphDev* g = ws->g;
+  if (root >= g->n) return set_error(NWG_EINVAL, "root " + std::to_string(root) + " >= n " + std::to_string(g->n));
+  if (alpha <= 0 || beta <= 0) return set_error(NWG_EINVAL, "alpha and beta must be positive");
+  const int rc = run_stepped(ws->params, g->sm_count, root, alpha, beta, parents ? parents : ws->parents, stream);
+  if (rc == NWG_OK) ws->ran = true;
+  return rc;
+}
+
+int zero_indegree_into(const uint64_t* in_off, uint64_t n, uint32_t* Z, int sm_count, cudaStream_t stream) {
+  const uint32_t nwords = (uint32_t)((n + 31) / 32);
+  if (nwords) {
+    k_zero_indegree<<<std::max(1, sm_count * 4), kThreads, 0, stream>>>(in_off, n, nwords, Z);
+    NWG_CUDA_TRY(cudaGetLastError());
+  }
   return NWG_OK;
 }
 

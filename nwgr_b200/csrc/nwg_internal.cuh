@@ -171,6 +171,9 @@ void ws_free(Workspace* ws);
 int  ws_launch(Workspace* ws, uint32_t root, int alpha, int beta, uint32_t* parents, cudaStream_t stream,
                bool topdown_only);
 int  ws_launch_stepped(Workspace* ws, uint32_t root, int alpha, int beta, uint32_t* parents, cudaStream_t stream);
+int  run_stepped(const DobfsParams& params, int sm_count, uint32_t root, int alpha, int beta, uint32_t* parents,
+                 cudaStream_t stream);
+int  zero_indegree_into(const uint64_t* in_off, uint64_t n, uint32_t* Z, int sm_count, cudaStream_t stream);
 void fill_stats(const Ctrl& c, nwg_bfs_stats* s);
 int  build_zero_indegree(GraphDev* g, cudaStream_t stream);
 int  component_edges(GraphDev* g, const uint32_t* parents, uint64_t* edges, uint64_t* vertices);
