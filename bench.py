@@ -157,6 +157,26 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def max_over_ranks(values, dist=None, device="cpu"):
+    """Element-wise maximum of a per-rank float64 vector over all ranks (the
+    slowest rank's time per root); identity without a process group."""
+    if dist is None:
+        return np.asarray(values, np.float64)
+    import torch
+
+    t = torch.tensor(np.asarray(values, np.float64), device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.cpu().numpy()
+
+
+def replica_gteps(e_r, per_root_ms, world):
+    """Whole-job throughput of `world` replicas that each traverse the same
+    roots: world x harmonic mean over roots of (E_r / 2) / t_r, t_r the
+    slowest rank's time for root r."""
+    gteps = (np.asarray(e_r, np.float64) / 2.0) / (np.asarray(per_root_ms, np.float64) * 1e-3) / 1e9
+    return world * hmean(gteps), gteps
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -319,13 +339,8 @@ def main():
     wall = time.perf_counter() - t0
     clk = clocks.stop()
 
-    per_root_ms = np.mean(np.asarray(rec), axis=0)  # mean over steps, per root
-    if dist:
-        t = torch.tensor(per_root_ms, device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        per_root_ms = t.cpu().numpy()
-    gteps = (e_r / 2.0) / (per_root_ms * 1e-3) / 1e9
-    value = world * hmean(gteps)
+    per_root_ms = max_over_ranks(np.mean(np.asarray(rec), axis=0), dist, "cuda")  # mean over steps, per root
+    value, gteps = replica_gteps(e_r, per_root_ms, world)
     hbm, hbm_kind = peaks()
     b_r = 4.0 * e_r + 8.0 * n_r + 4.0 * n
     achieved_gbs = float(np.mean(b_r / (per_root_ms * 1e-3)) / 1e9)

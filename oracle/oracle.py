@@ -59,6 +59,30 @@ def build_ref(force: bool = False) -> str | None:
     return REF_SO
 
 
+DROPIN_BIN = os.path.join(os.path.dirname(HERE), "tests", "cpp", "_build", "dropin_test")
+
+
+def build_dropin_test(force: bool = False) -> str | None:
+    """Compile tests/cpp/dropin_test.cpp: this repository's include/ first (the
+    drop-in nwgraph/algorithms/bfs.hpp and nwg_bfs.h), NWGraph's headers
+    second, the TBB-compatible shim for NWGraph's other headers, linked to
+    libnwgr_b200.so.  Needs the NWGraph sources; returns None without them."""
+    root = os.path.dirname(HERE)
+    src = os.path.join(root, "tests", "cpp", "dropin_test.cpp")
+    lib_dir = os.path.join(root, "nwgr_b200")
+    if not reference_available():
+        return DROPIN_BIN if os.path.exists(DROPIN_BIN) else None
+    deps = [src, os.path.join(root, "include", "nwgraph", "algorithms", "bfs.hpp"),
+            os.path.join(root, "include", "nwg_bfs.h")]
+    if force or not os.path.exists(DROPIN_BIN) or any(os.path.getmtime(d) > os.path.getmtime(DROPIN_BIN) for d in deps):
+        os.makedirs(os.path.dirname(DROPIN_BIN), exist_ok=True)
+        subprocess.check_call(
+            ["g++", "-std=c++20", "-O2", "-pthread", "-Wno-deprecated-declarations", "-I", os.path.join(root, "include"),
+             "-I", os.path.join(HERE, "tbb_compat"), "-I", REFERENCE_INCLUDE, src, "-o", DROPIN_BIN,
+             "-L", lib_dir, "-lnwgr_b200", "-Wl,-rpath,$ORIGIN/../../../nwgr_b200"])
+    return DROPIN_BIN
+
+
 class _Trace(C.Structure):
     _fields_ = [("cap", C.c_uint32), ("steps", C.c_uint32), ("dir", C.POINTER(C.c_uint8)),
                 ("frontier", C.POINTER(C.c_uint64)), ("found", C.POINTER(C.c_uint64)),
