@@ -64,6 +64,7 @@ def parse():
     ap.add_argument("--cpu-sample-roots", type=int, default=4)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--profile-one", action="store_true",
                     help="after warm-up, run one traversal inside an NVTX range 'nwg_profile' and exit (for ncu)")
     return ap.parse_args()
@@ -229,6 +230,64 @@ def run_reference_arm(args, spec, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def bench_batched(nwg, torch, scale=22, ks=(64, 256, 1024), reps=3):
+    """Batched multi-source BFS (64 sources per 64-bit word) against 64
+    back-to-back single-source traversals of the same roots, on RMAT-`scale`.
+    Aggregate GTEPS = sum over roots of E_r / 2, over the device time of the
+    whole batch (CUDA events); depths are checked equal on the host for a
+    sample of roots."""
+    g = nwg.Graph.rmat(scale, 16, seed=GRAPH_SEED)
+    kmax = max(ks)
+    roots = g.roots(kmax, seed=ROOT_SEED)
+    stream = torch.cuda.Stream()
+    par = torch.empty(g.n, dtype=torch.int32, device="cuda")
+    ws = g.workspace()
+    e_r = np.zeros(kmax)
+    for i, r in enumerate(roots):  # E_r of every root (untimed)
+        nwg.bfs_device(g, int(r), par)
+        e_r[i] = g.component_edges(par)[0]
+    # 64 back-to-back single-source traversals
+    plain = []
+    for rep in range(reps + 1):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            a.record(stream)
+            for r in roots[:64]:
+                ws.bfs_async(int(r), par, stream.cuda_stream)
+            b.record(stream)
+        stream.synchronize()
+        if rep:
+            plain.append(a.elapsed_time(b))
+    plain_ms = float(np.median(plain))
+    plain_gteps = float(e_r[:64].sum() / 2.0 / (plain_ms * 1e-3) / 1e9)
+    ms = nwg.MsWorkspace(g)
+    out = {"graph": f"RMAT-{scale} ef16", "plain64_ms": plain_ms, "plain64_gteps": plain_gteps, "msbfs": {}}
+    for k in ks:
+        depths = torch.empty((k, g.n), dtype=torch.uint8, device="cuda")
+        times = []
+        for rep in range(reps + 1):
+            st = ms.run(roots[:k], depths, stream=stream.cuda_stream)
+            if rep:
+                times.append(st.device_ms)
+        t = float(np.median(times))
+        gteps = float(e_r[:k].sum() / 2.0 / (t * 1e-3) / 1e9)
+        out["msbfs"][str(k)] = {"ms": t, "gteps": gteps, "vs_plain64": gteps / plain_gteps, "passes": st.passes,
+                                "push_levels": st.push_levels, "pull_levels": st.pull_levels}
+        if k == min(ks):  # depths equal to the single-source traversals for a sample of roots
+            d = depths.cpu().numpy()
+            ok = True
+            for i in (0, k // 2, k - 1):
+                nwg.bfs_device(g, int(roots[i]), par)
+                dd = nwg.depths_from_parents(par.cpu().numpy().view(np.uint32), int(roots[i]))
+                ok &= bool(np.array_equal(np.where(dd == 0xFFFFFFFF, 255, dd).astype(np.uint8), d[i]))
+            out["depths_match_single_source_sample"] = ok
+        del depths
+    ms.close()
+    ws.close()
+    g.release()
+    return out
+
+
 def cpu_baseline(off, cols, roots, n_roots):
     """Reference bfs.hpp on the host cores over a bounded sample of roots."""
     from oracle.oracle import Reference
@@ -371,8 +430,16 @@ def main():
                "d2h_bytes_per_step": int(4 * n * len(roots)),
                "note": "per step: upload CSR from pinned host memory, 64 nwg_bfs calls each returning parents "
                        "to pinned host memory, release"}
+    batched = None
+    if not args.no_batched:
+        ws.close()
+        g.release()
+        ws, g = None, None
+        batched = bench_batched(nwg, torch)
     cpu = None
     if rank == 0 and not args.no_cpu:
+        if g is None:
+            g = make_graph(nwg, spec)
         off, cols = g.csr()
         cpu = cpu_baseline(off, cols, roots, args.cpu_sample_roots)
 
@@ -393,11 +460,13 @@ def main():
                          "algorithmic_bytes_per_launch_mean": float(np.mean(b_r)),
                          "traffic": float(traffic) if traffic else None},
             "gpu_launches": int(np.sum(launches)) * args.steps,
-            "clocks": clk, "e2e": e2e, "cpu_baseline": cpu,
+            "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, "batched": batched,
         }
         print(json.dumps(line), flush=True)
-    ws.close()
-    g.release()
+    if ws is not None:
+        ws.close()
+    if g is not None:
+        g.release()
     if dist:
         dist.destroy_process_group()
 

@@ -139,6 +139,38 @@ int nwg_component_edges(nwg_graph g, const uint32_t* parents_dev, uint64_t* edge
  * host arrays of the sizes nwg_graph_info reports; any pointer may be NULL. */
 int nwg_graph_copy_csr(nwg_graph g, uint64_t* out_off, uint32_t* out_col, uint64_t* in_off, uint32_t* in_col);
 
+/* Batched multi-source BFS (no reference counterpart: NWGraph's bfs is
+ * single-source; the result equals one single-source BFS per root).  Sources
+ * are packed 64 per 64-bit word, up to 256 per pass; each level pushes
+ * (top-down, 64-bit atomicOr) or pulls (bottom-up, no atomics) by the rule
+ * of nw::graph::bfs: pull when the frontier's out-edges exceed the
+ * unexplored edges / alpha (4 suits it better than the single-source 15: a
+ * multi-source pull rarely stops early).  depths_dev is a device array [k][n] of
+ * uint8: depth of vertex v from root i at depths_dev[i * n + v], 255 =
+ * unreached; NWG_EOVERFLOW if some depth would be >= 255.  Runs on `stream`
+ * (NULL = the workspace's own stream) and returns when done. */
+typedef struct nwg_msbfs_ws_s* nwg_msbfs_ws;
+#define NWG_MS_TRACE_CAP 64
+typedef struct {
+  int32_t status;
+  uint32_t passes;      /* passes of up to 256 sources */
+  uint32_t levels;      /* maximum depth + 1 over all sources */
+  uint32_t push_levels; /* levels run top-down, summed over passes */
+  uint32_t pull_levels; /* levels run bottom-up, summed over passes */
+  float device_ms;      /* device time (CUDA events) */
+  /* the first pass's levels: direction (0 push, 1 pull), device time,
+   * out-edges of the level's frontier, (source, vertex) pairs discovered */
+  uint32_t trace_len;
+  uint8_t trace_pull[NWG_MS_TRACE_CAP];
+  float trace_ms[NWG_MS_TRACE_CAP];
+  uint64_t trace_frontier_edges[NWG_MS_TRACE_CAP];
+  uint64_t trace_discovered[NWG_MS_TRACE_CAP];
+} nwg_msbfs_stats;
+int nwg_msbfs_ws_create(nwg_graph g, nwg_msbfs_ws* out);
+int nwg_msbfs_ws_destroy(nwg_msbfs_ws ws);
+int nwg_msbfs(nwg_msbfs_ws ws, const uint32_t* roots_host, uint32_t k, uint8_t* depths_dev, int alpha, void* stream,
+              nwg_msbfs_stats* stats);
+
 /* Direction-optimizing BFS that allocates no device memory.  No counterpart
  * in the reference: NWGraph's bfs allocates its state per call.  For callers
  * that may not call cudaMalloc/cudaFree (both synchronise the device; latency-

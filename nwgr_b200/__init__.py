@@ -38,7 +38,8 @@ EXPORTED = (
     "nwg_version", "nwg_last_error", "nwg_graph_register", "nwg_graph_register_u32off", "nwg_graph_release",
     "nwg_graph_info", "nwg_bfs", "nwg_ws_create", "nwg_ws_destroy", "nwg_bfs_async", "nwg_ws_stats",
     "nwg_bfs_topdown", "nwg_bfs_stepped", "nwg_component_edges", "nwg_graph_copy_csr", "nwg_gen_rmat", "nwg_gen_uniform",
-    "nwg_gen_grid", "nwg_pick_roots", "nwg_bfs_noalloc",
+    "nwg_gen_grid", "nwg_pick_roots", "nwg_bfs_noalloc", "nwg_msbfs_ws_create", "nwg_msbfs_ws_destroy",
+    "nwg_msbfs",
 )
 
 
@@ -72,6 +73,28 @@ class Stats(C.Structure):
         return np.diff(np.concatenate([[int(self.first_decide_ns)], end]))
 
 
+MS_TRACE_CAP = 64
+# Direction switch of the multi-source BFS: a level pulls when its frontier's
+# out-edges exceed the unexplored edges / MS_ALPHA.  Lower than the
+# single-source alpha (15): a multi-source pull ORs every in-edge of a vertex
+# until all sources have reached it, so it rarely stops early.
+MS_ALPHA = 4
+
+
+class MsStats(C.Structure):
+    _fields_ = [("status", C.c_int32), ("passes", C.c_uint32), ("levels", C.c_uint32),
+                ("push_levels", C.c_uint32), ("pull_levels", C.c_uint32), ("device_ms", C.c_float),
+                ("trace_len", C.c_uint32), ("trace_pull", C.c_uint8 * MS_TRACE_CAP),
+                ("trace_ms", C.c_float * MS_TRACE_CAP), ("trace_frontier_edges", C.c_uint64 * MS_TRACE_CAP),
+                ("trace_discovered", C.c_uint64 * MS_TRACE_CAP)]
+
+    def trace(self):
+        k = self.trace_len
+        return [{"pull": int(self.trace_pull[i]), "ms": float(self.trace_ms[i]),
+                 "frontier_edges": int(self.trace_frontier_edges[i]), "discovered": int(self.trace_discovered[i])}
+                for i in range(k)]
+
+
 _vp = C.c_void_p
 _u32, _u64, _int = C.c_uint32, C.c_uint64, C.c_int
 
@@ -101,6 +124,9 @@ def _load():
         "nwg_gen_grid": (_int, [_u32, _u32, _u32, _u64, C.POINTER(_vp)]),
         "nwg_pick_roots": (_int, [_vp, _u64, _u32, _vp]),
         "nwg_bfs_noalloc": (_int, [_vp, _vp, _vp, _vp, _u64, _u32, _int, _int, _vp, _vp]),
+        "nwg_msbfs_ws_create": (_int, [_vp, C.POINTER(_vp)]),
+        "nwg_msbfs_ws_destroy": (_int, [_vp]),
+        "nwg_msbfs": (_int, [_vp, _vp, _u32, _vp, _int, _vp, C.POINTER(MsStats)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -233,6 +259,44 @@ class Graph:
                 self.h = None
         except Exception:
             pass
+
+
+class MsWorkspace:
+    """State of the batched multi-source BFS (nwg_msbfs_ws)."""
+
+    def __init__(self, g: Graph):
+        self.g = g
+        h = _vp()
+        check(lib.nwg_msbfs_ws_create(g.h, C.byref(h)))
+        self.h = h.value
+
+    def run(self, roots, depths_dev, alpha: int = MS_ALPHA, stream=None) -> MsStats:
+        """Depths of every vertex from every root into depths_dev (device
+        uint8 [k][n]; 255 = unreached).  Returns the MsStats."""
+        roots = np.ascontiguousarray(roots, dtype=np.uint32)
+        st = MsStats()
+        check(lib.nwg_msbfs(self.h, roots.ctypes.data, roots.size, _ptr(depths_dev), alpha, _ptr(stream), C.byref(st)))
+        return st
+
+    def close(self):
+        if self.h and self.g.h:
+            check(lib.nwg_msbfs_ws_destroy(self.h))
+        self.h = None
+
+
+def msbfs(g: Graph, roots, alpha: int = MS_ALPHA):
+    """Batched multi-source BFS; returns host uint8 depths [k][n] (255 =
+    unreached) and the MsStats.  Uses torch for the device output buffer."""
+    import torch
+
+    roots = np.ascontiguousarray(roots, dtype=np.uint32)
+    out = torch.empty((roots.size, g.n), dtype=torch.uint8, device="cuda")
+    ws = MsWorkspace(g)
+    try:
+        st = ws.run(roots, out, alpha)
+    finally:
+        ws.close()
+    return out.cpu().numpy(), st
 
 
 class Workspace:

@@ -69,6 +69,8 @@ void graph_free(GraphDev* g) {
   DeviceGuard dg(g->device);
   for (Workspace* ws : g->workspaces) ws_free(ws);
   g->workspaces.clear();
+  for (MsWorkspace* ws : g->ms_workspaces) ms_ws_free(ws);
+  g->ms_workspaces.clear();
   g->default_ws = nullptr;
   if (g->owns_out) {
     cudaFree(g->off);
@@ -415,6 +417,56 @@ NWG_API int nwg_ws_stats(nwg_bfs_ws h, nwg_bfs_stats* stats) {
   fill_stats(*ws->ctrl_host, stats);
   stats->device_ms = 0.f;
   return NWG_OK;
+  NWG_GUARD_END
+}
+
+NWG_API int nwg_msbfs_ws_create(nwg_graph h, nwg_msbfs_ws* out) {
+  NWG_GUARD_BEGIN
+  if (!h || !out) return set_error(NWG_EINVAL, "NULL argument");
+  auto*                       g = reinterpret_cast<GraphDev*>(h);
+  std::lock_guard<std::mutex> lk(g->mu);
+  DeviceGuard                 dg(g->device);
+  auto*                       ws = new MsWorkspace();
+  int                         rc = ms_ws_init(g, ws);
+  if (rc) {
+    ms_ws_free(ws);
+    return rc;
+  }
+  g->ms_workspaces.push_back(ws);
+  *out = reinterpret_cast<nwg_msbfs_ws>(ws);
+  return NWG_OK;
+  NWG_GUARD_END
+}
+
+NWG_API int nwg_msbfs_ws_destroy(nwg_msbfs_ws h) {
+  NWG_GUARD_BEGIN
+  if (!h) return set_error(NWG_EINVAL, "NULL workspace");
+  auto*                       ws = reinterpret_cast<MsWorkspace*>(h);
+  GraphDev*                   g  = ws->g;
+  std::lock_guard<std::mutex> lk(g->mu);
+  DeviceGuard                 dg(g->device);
+  g->ms_workspaces.erase(std::remove(g->ms_workspaces.begin(), g->ms_workspaces.end(), ws), g->ms_workspaces.end());
+  ms_ws_free(ws);
+  return NWG_OK;
+  NWG_GUARD_END
+}
+
+NWG_API int nwg_msbfs(nwg_msbfs_ws h, const uint32_t* roots_host, uint32_t k, uint8_t* depths_dev, int alpha,
+                      void* stream, nwg_msbfs_stats* stats) {
+  NWG_GUARD_BEGIN
+  if (!h || (!roots_host && k) || (!depths_dev && k)) return set_error(NWG_EINVAL, "NULL argument");
+  auto*           ws = reinterpret_cast<MsWorkspace*>(h);
+  DeviceGuard     dg(ws->g->device);
+  nwg_msbfs_stats st = {};
+  cudaStream_t    s  = stream ? reinterpret_cast<cudaStream_t>(stream) : ws->stream;
+  NWG_CUDA_TRY(cudaEventRecord(ws->ev0, s));
+  int rc = ms_run(ws, roots_host, k, depths_dev, alpha, s, &st);
+  NWG_CUDA_TRY(cudaEventRecord(ws->ev1, s));
+  NWG_CUDA_TRY(cudaEventSynchronize(ws->ev1));
+  cudaEventElapsedTime(&st.device_ms, ws->ev0, ws->ev1);
+  st.status = rc;
+  if (stats) *stats = st;
+  return rc;
   NWG_GUARD_END
 }
 

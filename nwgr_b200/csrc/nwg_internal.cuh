@@ -140,6 +140,23 @@ struct Workspace {
   bool            timed = false;
 };
 
+// State of the batched multi-source BFS (nwg_msbfs.cu); sized for 256
+// sources (four 64-bit words) per vertex.
+struct MsWorkspace {
+  GraphDev*    g       = nullptr;
+  uint64_t*    vis     = nullptr;
+  uint64_t*    fr[2]   = {nullptr, nullptr};
+  uint64_t*    nx      = nullptr;
+  uint64_t*    list[2] = {nullptr, nullptr};  // frontier chunk entries
+  uint64_t     list_cap = 0;
+  void*        cnt     = nullptr;
+  uint32_t*    roots   = nullptr;
+  uint32_t*    roots_uniq = nullptr;
+  cudaStream_t stream  = nullptr;
+  cudaEvent_t  ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t  ev_lvl[2] = {nullptr, nullptr};
+};
+
 struct GraphDev {
   int       device = 0;
   uint64_t  n = 0, m = 0, in_m = 0;
@@ -151,9 +168,10 @@ struct GraphDev {
   bool      owns_out = false, owns_in = false, symmetric = true;
   int       sm_count = 148;
   Thresholds th{32, 256, 8};
-  std::mutex              mu;
-  Workspace*              default_ws = nullptr;
-  std::vector<Workspace*> workspaces;
+  std::mutex                mu;
+  Workspace*                default_ws = nullptr;
+  std::vector<Workspace*>   workspaces;
+  std::vector<MsWorkspace*> ms_workspaces;
 };
 
 // Error plumbing (nwg_api.cu).
@@ -178,6 +196,12 @@ void fill_stats(const Ctrl& c, nwg_bfs_stats* s);
 int  build_zero_indegree(GraphDev* g, cudaStream_t stream);
 int  component_edges(GraphDev* g, const uint32_t* parents, uint64_t* edges, uint64_t* vertices);
 int  widen_offsets(const uint32_t* src, uint64_t* dst, uint64_t count, cudaStream_t stream);
+
+// nwg_msbfs.cu
+int  ms_ws_init(GraphDev* g, MsWorkspace* ws);
+void ms_ws_free(MsWorkspace* ws);
+int  ms_run(MsWorkspace* ws, const uint32_t* roots_host, uint32_t k, uint8_t* depths_dev, int alpha, cudaStream_t stream,
+            nwg_msbfs_stats* st);
 
 // nwg_gen.cu
 int gen_rmat(uint32_t scale, uint32_t ef, uint64_t seed, uint32_t ta, uint32_t tab, uint32_t tabc, GraphDev* g);
