@@ -65,6 +65,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-ragged", action="store_true")
     ap.add_argument("--profile-one", action="store_true",
                     help="after warm-up, run one traversal inside an NVTX range 'nwg_profile' and exit (for ncu)")
     return ap.parse_args()
@@ -288,6 +289,48 @@ def bench_batched(nwg, torch, scale=22, ks=(64, 256, 1024), reps=3):
     return out
 
 
+def bench_ragged(nwg, torch, num_graphs=1000, reps=3):
+    """Ragged batch: num_graphs graphs (n log-uniform on 2^10..2^18, half
+    RMAT with edge factor 8..32, half 2D grids with 1% shortcuts), 4 roots
+    each, all (graph, root) items in one persistent launch replayed as a CUDA
+    graph, parameters from the autotuner (cached per graph-shape class).
+    Compared with the same items as one nwg_bfs call each on separately
+    registered graphs (device time of the calls summed)."""
+    from nwgr_b200.ragged import Autotuner, ragged_workload
+
+    t0 = time.perf_counter()
+    graphs, mn, roots, kinds = ragged_workload(nwg, num_graphs)
+    gen_s = time.perf_counter() - t0
+    batch = nwg.RaggedBatch(graphs)
+    tuner = Autotuner()
+    t0 = time.perf_counter()
+    params, bps = tuner.tune(batch, mn, roots)
+    tune_s = time.perf_counter() - t0
+    items = Autotuner.items(mn, roots, params)
+    parents, offs, res, _ = batch.run(items, blocks_per_sm=bps)
+    times = [batch.run(items, parents_dev=parents, blocks_per_sm=bps)[3] for _ in range(reps)]
+    t = float(np.median(times))
+    host = parents.cpu().numpy().view(np.uint32)
+    e_total = 0.0
+    for i, (g, r, *_rest) in enumerate(items):
+        off = graphs[g][0]
+        p = host[offs[i]:offs[i] + off.size - 1]
+        e_total += float((off[1:] - off[:-1])[p != 0xFFFFFFFF].sum())
+    per_call_ms = 0.0
+    for g, (off, cols) in enumerate(graphs):
+        G = nwg.Graph.from_csr(off, cols)
+        for r in roots[g]:
+            _, st = nwg.bfs(G, G, int(r), stats=True)
+            per_call_ms += st.device_ms
+        G.release()
+    batch.release()
+    return {"graphs": num_graphs, "items": len(items), "total_vertices": int(sum(n for n, _ in mn)),
+            "total_entries": int(sum(m for _, m in mn)), "persistent_ms": t,
+            "gteps": e_total / 2.0 / (t * 1e-3) / 1e9, "per_call_device_ms_sum": per_call_ms,
+            "speedup_vs_per_call": per_call_ms / t, "blocks_per_sm": bps,
+            "classes": {k: v.__dict__ for k, v in params.items()}, "generate_s": gen_s, "autotune_s": tune_s}
+
+
 def cpu_baseline(off, cols, roots, n_roots):
     """Reference bfs.hpp on the host cores over a bounded sample of roots."""
     from oracle.oracle import Reference
@@ -436,6 +479,13 @@ def main():
         g.release()
         ws, g = None, None
         batched = bench_batched(nwg, torch)
+    ragged = None
+    if not args.no_ragged:
+        if ws is not None:
+            ws.close()
+            g.release()
+            ws, g = None, None
+        ragged = bench_ragged(nwg, torch)
     cpu = None
     if rank == 0 and not args.no_cpu:
         if g is None:
@@ -460,7 +510,7 @@ def main():
                          "algorithmic_bytes_per_launch_mean": float(np.mean(b_r)),
                          "traffic": float(traffic) if traffic else None},
             "gpu_launches": int(np.sum(launches)) * args.steps,
-            "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, "batched": batched,
+            "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, "batched": batched, "ragged": ragged,
         }
         print(json.dumps(line), flush=True)
     if ws is not None:

@@ -171,6 +171,41 @@ int nwg_msbfs_ws_destroy(nwg_msbfs_ws ws);
 int nwg_msbfs(nwg_msbfs_ws ws, const uint32_t* roots_host, uint32_t k, uint8_t* depths_dev, int alpha, void* stream,
               nwg_msbfs_stats* stats);
 
+/* Ragged batch: many small graphs packed in HBM once, and a table of
+ * (graph, root) traversals run in ONE persistent launch (replayed as a CUDA
+ * graph).  Each block of the launch takes items from a device work counter
+ * and runs an item's whole direction-optimizing level loop by itself, with
+ * the item's own alpha, beta and degree threshold (warp_min, 32..256; 0 =
+ * 32) -- the values the autotuner picks per graph-shape class.  No reference
+ * counterpart beyond one nw::graph::bfs call per item; results are the same.
+ * Registration: graph g has graph_n[g] vertices; off_concat holds each
+ * graph's n + 1 offsets (starting at 0) one graph after the other, col_concat
+ * each graph's columns one after the other; all host arrays, validated. */
+typedef struct nwg_ragged_s* nwg_ragged;
+typedef struct {
+  uint32_t graph;
+  uint32_t root;
+  int32_t alpha;
+  int32_t beta;
+  uint32_t warp_min;
+} nwg_ragged_item;
+typedef struct {
+  int32_t status;
+  uint32_t steps, levels, td_steps, bu_steps, b2q_steps;
+  uint64_t reached;
+} nwg_ragged_result;
+int nwg_ragged_register(uint32_t num_graphs, const uint64_t* graph_n, const uint64_t* off_concat,
+                        const uint32_t* col_concat, nwg_ragged* out);
+int nwg_ragged_release(nwg_ragged r);
+int nwg_ragged_info(nwg_ragged r, uint32_t* num_graphs, uint64_t* total_n, uint64_t* nmax, uint64_t* mmax);
+/* parents_dev: packed output, item i's parents (n of its graph) start at
+ * item_offsets_host[i] (the running sum of the items' n, written when
+ * non-NULL).  blocks_per_sm: resident blocks per SM of the persistent launch
+ * (1..8, 0 = 2).  Synchronous; device_ms = device time of the launch. */
+int nwg_ragged_bfs(nwg_ragged r, uint32_t num_items, const nwg_ragged_item* items, uint32_t* parents_dev,
+                   uint64_t* item_offsets_host, nwg_ragged_result* results_host, uint32_t blocks_per_sm,
+                   float* device_ms);
+
 /* Direction-optimizing BFS that allocates no device memory.  No counterpart
  * in the reference: NWGraph's bfs allocates its state per call.  For callers
  * that may not call cudaMalloc/cudaFree (both synchronise the device; latency-

@@ -39,7 +39,7 @@ EXPORTED = (
     "nwg_graph_info", "nwg_bfs", "nwg_ws_create", "nwg_ws_destroy", "nwg_bfs_async", "nwg_ws_stats",
     "nwg_bfs_topdown", "nwg_bfs_stepped", "nwg_component_edges", "nwg_graph_copy_csr", "nwg_gen_rmat", "nwg_gen_uniform",
     "nwg_gen_grid", "nwg_pick_roots", "nwg_bfs_noalloc", "nwg_msbfs_ws_create", "nwg_msbfs_ws_destroy",
-    "nwg_msbfs",
+    "nwg_msbfs", "nwg_ragged_register", "nwg_ragged_release", "nwg_ragged_info", "nwg_ragged_bfs",
 )
 
 
@@ -95,6 +95,16 @@ class MsStats(C.Structure):
                 for i in range(k)]
 
 
+class RaggedItem(C.Structure):
+    _fields_ = [("graph", C.c_uint32), ("root", C.c_uint32), ("alpha", C.c_int32), ("beta", C.c_int32),
+                ("warp_min", C.c_uint32)]
+
+
+class RaggedResult(C.Structure):
+    _fields_ = [("status", C.c_int32), ("steps", C.c_uint32), ("levels", C.c_uint32), ("td_steps", C.c_uint32),
+                ("bu_steps", C.c_uint32), ("b2q_steps", C.c_uint32), ("reached", C.c_uint64)]
+
+
 _vp = C.c_void_p
 _u32, _u64, _int = C.c_uint32, C.c_uint64, C.c_int
 
@@ -127,6 +137,10 @@ def _load():
         "nwg_msbfs_ws_create": (_int, [_vp, C.POINTER(_vp)]),
         "nwg_msbfs_ws_destroy": (_int, [_vp]),
         "nwg_msbfs": (_int, [_vp, _vp, _u32, _vp, _int, _vp, C.POINTER(MsStats)]),
+        "nwg_ragged_register": (_int, [_u32, _vp, _vp, _vp, C.POINTER(_vp)]),
+        "nwg_ragged_release": (_int, [_vp]),
+        "nwg_ragged_info": (_int, [_vp, C.POINTER(_u32), C.POINTER(_u64), C.POINTER(_u64), C.POINTER(_u64)]),
+        "nwg_ragged_bfs": (_int, [_vp, _u32, _vp, _vp, _vp, _vp, _u32, C.POINTER(C.c_float)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -297,6 +311,53 @@ def msbfs(g: Graph, roots, alpha: int = MS_ALPHA):
     finally:
         ws.close()
     return out.cpu().numpy(), st
+
+
+class RaggedBatch:
+    """Many small CSR graphs packed in HBM (nwg_ragged) and traversed as a
+    table of (graph, root) items in one persistent launch."""
+
+    def __init__(self, graphs):
+        """graphs: sequence of (offsets uint64[n+1], columns uint32[m])."""
+        ns = np.asarray([g[0].size - 1 for g in graphs], np.uint64)
+        off = np.ascontiguousarray(np.concatenate([np.asarray(g[0], np.uint64) for g in graphs]))
+        cols = np.ascontiguousarray(np.concatenate([np.asarray(g[1], np.uint32) for g in graphs]))
+        h = _vp()
+        check(lib.nwg_ragged_register(ns.size, ns.ctypes.data, off.ctypes.data, cols.ctypes.data, C.byref(h)))
+        self.h = h.value
+        self.n = ns
+        self.num_graphs = ns.size
+
+    def run(self, items, parents_dev=None, blocks_per_sm: int = 2):
+        """items: list of (graph, root, alpha, beta, warp_min).  Returns
+        (parents packed as a device tensor, item offsets, results, device ms)."""
+        import torch
+
+        k = len(items)
+        arr = (RaggedItem * k)(*[RaggedItem(int(g), int(r), int(a), int(b), int(w)) for g, r, a, b, w in items])
+        # sizes of valid items only: the C layer rejects bad ones with a message
+        total = int(sum(int(self.n[g]) for g, *_ in items if 0 <= int(g) < self.num_graphs))
+        if parents_dev is None:
+            parents_dev = torch.empty(max(total, 1), dtype=torch.int32, device="cuda")
+        offs = np.zeros(k, np.uint64)
+        res = (RaggedResult * k)()
+        ms = C.c_float(0.0)
+        check(lib.nwg_ragged_bfs(self.h, k, arr, _ptr(parents_dev), offs.ctypes.data, res, int(blocks_per_sm),
+                                 C.byref(ms)))
+        return parents_dev, offs, res, ms.value
+
+    def release(self):
+        if self.h:
+            check(lib.nwg_ragged_release(self.h))
+            self.h = None
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib.nwg_ragged_release(self.h)
+                self.h = None
+        except Exception:
+            pass
 
 
 class Workspace:

@@ -445,11 +445,11 @@ __device__ __forceinline__ void gather_ranges(const DobfsParams& p, uint32_t* __
 // ---------------------------------------------------------------------------
 // k_init: parents := null except root (bfs.hpp:175,180), V := {root},
 // control block := the reference's initial state (bfs.hpp:166-181).
-__global__ void __launch_bounds__(kThreads) k_init(DobfsParams p, uint32_t root, uint32_t alpha, uint32_t beta,
-                                                   uint32_t* parents, uint32_t topdown_only) {
+__device__ __forceinline__ void init_step(const DobfsParams& p, uint32_t root, uint32_t alpha, uint32_t beta,
+                                          uint32_t* parents, uint32_t topdown_only, uint32_t block, uint32_t nblocks) {
   const uint64_t n      = p.n;
-  const uint64_t tid    = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t tid    = (uint64_t)block * blockDim.x + threadIdx.x;
+  const uint64_t stride = (uint64_t)nblocks * blockDim.x;
   if ((reinterpret_cast<uintptr_t>(parents) & 15) == 0) {
     const uint64_t n4 = n >> 2;
     uint4*         p4 = reinterpret_cast<uint4*>(parents);
@@ -517,6 +517,11 @@ __global__ void __launch_bounds__(kThreads) k_init(DobfsParams p, uint32_t root,
     const uint64_t cap = 2 * n + 64;
     c.max_steps = cap > 0xFFFFFF00ull ? 0xFFFFFF00u : (uint32_t)cap;
   }
+}
+
+__global__ void __launch_bounds__(kThreads) k_init(DobfsParams p, uint32_t root, uint32_t alpha, uint32_t beta,
+                                                   uint32_t* parents, uint32_t topdown_only) {
+  init_step(p, root, alpha, beta, parents, topdown_only, blockIdx.x, gridDim.x);
 }
 
 __device__ __forceinline__ uint64_t frontier_size(const CtrlHdr& c, uint32_t qi) {
@@ -839,7 +844,7 @@ __device__ __forceinline__ uint32_t compact_tile(uint32_t bits, uint16_t* list) 
 // kBuProbe per round with independent loads; lanes still unresolved with
 // edges left are scanned by the whole warp, 32 in-edges per step.  The first hit in row order becomes the parent, exactly as the
 // reference's sequential scan with `break`.
-__global__ void __launch_bounds__(kThreads) k_bu(DobfsParams p) {
+__device__ __forceinline__ void bu_step(const DobfsParams& p, uint32_t block, uint32_t nblocks) {
   __shared__ uint16_t s_cand[kWarps][kBuTileWords * 32];
   __shared__ uint32_t s_new[kWarps][kBuTileWords];
   CtrlHdr*        c       = &p.ctrl->h;
@@ -856,8 +861,8 @@ __global__ void __launch_bounds__(kThreads) k_bu(DobfsParams p) {
   const uint64_t  ntiles  = (p.nwords + kBuTileWords - 1) / kBuTileWords;
   uint32_t        awake   = 0;
 
-  const uint64_t  gwarp   = (uint64_t)blockIdx.x * kWarps + wib;
-  const uint64_t  nwarps  = (uint64_t)gridDim.x * kWarps;
+  const uint64_t  gwarp   = (uint64_t)block * kWarps + wib;
+  const uint64_t  nwarps  = (uint64_t)nblocks * kWarps;
   for (uint64_t t = gwarp; t < ntiles; t += nwarps) {
     const uint64_t w  = t * kBuTileWords + lane;
     const bool     wv = lane < kBuTileWords && w < p.nwords;
@@ -949,20 +954,21 @@ __global__ void __launch_bounds__(kThreads) k_bu(DobfsParams p) {
   if (threadIdx.x == 0 && tot) atomicAdd(&c->acc_awake, (unsigned long long)tot);
 }
 
+__global__ void __launch_bounds__(kThreads) k_bu(DobfsParams p) { bu_step(p, blockIdx.x, gridDim.x); }
+
 // ---------------------------------------------------------------------------
 // k_b2q: bitmap -> queue (bfs.hpp:235-239) from C[bm], folding C[bm] into V
 // on the way.  Each warp compacts tiles of 32 words into its vertex buffer;
 // full buffers are appended per warp, the rest once per block at the end.
-__global__ void __launch_bounds__(kThreads) k_b2q(DobfsParams p) {
+__device__ __forceinline__ void b2q_step(const DobfsParams& p, TdWarp* s_tw, uint32_t block, uint32_t nblocks) {
   __shared__ uint16_t s_list[kWarps][kTileWords * 32];
-  __shared__ TdWarp   s_tw[kWarps];
   CtrlHdr*           c      = &p.ctrl->h;
   const uint32_t*    Cs     = c->bm ? p.C1 : p.C0;
   const uint32_t     qi     = c->cur;
   const unsigned     lane   = threadIdx.x & 31;
   const unsigned     wib    = threadIdx.x >> 5;
-  const uint64_t     gwarp  = (uint64_t)blockIdx.x * kWarps + wib;
-  const uint64_t     nwarps = (uint64_t)gridDim.x * kWarps;
+  const uint64_t     gwarp  = (uint64_t)block * kWarps + wib;
+  const uint64_t     nwarps = (uint64_t)nblocks * kWarps;
   const uint64_t     ntiles = (p.nwords + kTileWords - 1) / kTileWords;
   uint16_t* const    list   = s_list[wib];
   TdWarp&            tw     = s_tw[wib];
@@ -985,6 +991,11 @@ __global__ void __launch_bounds__(kThreads) k_b2q(DobfsParams p) {
   flush_block(p, s_tw, wcnt, qi, scout, nbig, false);
   const uint32_t nb = block_sum(nbig);
   if (threadIdx.x == 0 && nb) atomicAdd(&c->qbig[qi], nb);
+}
+
+__global__ void __launch_bounds__(kThreads) k_b2q(DobfsParams p) {
+  __shared__ TdWarp s_tw[kWarps];
+  b2q_step(p, s_tw, blockIdx.x, gridDim.x);
 }
 
 // In-degree-zero bitmap; bits past n are set so they are never candidates.
@@ -1023,6 +1034,120 @@ __global__ void k_component(const uint64_t* __restrict__ off, const uint32_t* __
 __global__ void k_widen(const uint32_t* __restrict__ src, uint64_t* __restrict__ dst, uint64_t count) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (uint64_t)gridDim.x * blockDim.x)
     dst[i] = src[i];
+}
+
+// ---------------------------------------------------------------------------
+// k_ragged: a ragged batch of (graph, root) traversals over many small packed
+// graphs in one persistent launch.  Each block takes items from an atomic
+// counter and runs the whole level loop of one item by itself: the same
+// init / decide / top-down / bottom-up / bitmap->queue steps as the
+// single-graph path, with nblocks = 1 and __syncthreads() in place of
+// kernel boundaries, in a scratch slot of its own.  No block ever waits on
+// another.
+constexpr uint64_t kAlign = 256;
+__host__ __device__ inline uint64_t al(uint64_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
+
+struct SlotLayout {
+  uint64_t ctrl, bits, qs, qc, bytes, qs_cap, qc_cap, nwords;
+};
+
+__host__ __device__ inline SlotLayout slot_layout(uint64_t nmax, uint64_t mmax) {
+  SlotLayout L;
+  L.nwords  = (nmax + 31) / 32;
+  L.qs_cap  = nmax > 0 ? nmax : 1;
+  const uint64_t big = (mmax / 32) < nmax ? (mmax / 32) : nmax;  // warp_min >= 32 in the ragged path
+  L.qc_cap  = mmax / 256 + big + 1;
+  L.ctrl    = 0;
+  L.bits    = al(sizeof(Ctrl));
+  L.qs      = al(L.bits + 3 * L.nwords * 4);
+  L.qc      = al(L.qs + 2 * L.qs_cap * 4);
+  L.bytes   = al(L.qc + 2 * L.qc_cap * 8);
+  return L;
+}
+
+__global__ void __launch_bounds__(kThreads) k_ragged(RaggedParams rp) {
+  __shared__ TdWarp   s_tw[kWarps];
+  __shared__ uint32_t s_item, s_next;
+  const SlotLayout    L    = slot_layout(rp.nmax, rp.mmax);
+  unsigned char*      slot = rp.scratch + (uint64_t)blockIdx.x * rp.slot_bytes;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(rp.next_item, 1u);
+    __syncthreads();
+    const uint32_t it = s_item;
+    __syncthreads();
+    if (it >= rp.n_items) break;
+    const RaggedItem  item = rp.items[it];
+    const RaggedGraph gr   = rp.graphs[item.graph];
+    DobfsParams       p    = {};
+    p.off                  = rp.off + gr.off_base;
+    p.col                  = rp.col + gr.col_base;
+    p.in_off               = p.off;
+    p.in_col               = p.col;
+    p.n                    = gr.n;
+    p.m                    = gr.m;
+    p.nwords               = (uint32_t)((gr.n + 31) / 32);
+    uint32_t* bits         = reinterpret_cast<uint32_t*>(slot + L.bits);
+    p.V                    = bits;
+    p.C0                   = bits + L.nwords;
+    p.C1                   = bits + 2 * L.nwords;
+    p.Z                    = rp.Z + gr.z_base;
+    uint32_t* qs           = reinterpret_cast<uint32_t*>(slot + L.qs);
+    uint64_t* qc           = reinterpret_cast<uint64_t*>(slot + L.qc);
+    p.qs[0]                = qs;
+    p.qs[1]                = qs + L.qs_cap;
+    p.qc[0]                = qc;
+    p.qc[1]                = qc + L.qc_cap;
+    p.qs_cap               = L.qs_cap;
+    p.qc_cap               = L.qc_cap;
+    p.th                   = Thresholds{item.warp_min, 256, 8};
+    p.ctrl                 = reinterpret_cast<Ctrl*>(slot + L.ctrl);
+    p.set_cond             = 0;
+    init_step(p, item.root, (uint32_t)item.alpha, (uint32_t)item.beta, rp.parents + item.out_base, 0u, 0, 1);
+    __syncthreads();
+    for (;;) {
+      if (threadIdx.x == 0) s_next = decide_core(p);
+      __syncthreads();
+      const uint32_t next = s_next;
+      if (next == kActNone) break;
+      if (next == kActBU) {
+        bu_step(p, 0, 1);
+      } else if (next == kActB2Q) {
+        b2q_step(p, s_tw, 0, 1);
+      } else {
+        td_step(p, s_tw, 0, 1);
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      const CtrlHdr& c = p.ctrl->h;
+      RaggedResult   r;
+      r.status    = c.status ? c.status : p.ctrl->err;
+      r.steps     = c.steps;
+      r.levels    = c.levels;
+      r.td_steps  = c.td_steps;
+      r.bu_steps  = c.bu_steps;
+      r.b2q_steps = c.b2q_steps;
+      r.reached   = c.reached;
+      rp.results[it] = r;
+    }
+    __syncthreads();
+  }
+}
+
+// In-degree-zero bitmaps of every packed graph (bits past n set).
+__global__ void k_zero_indegree_packed(const uint64_t* __restrict__ off, const RaggedGraph* __restrict__ graphs,
+                                       uint32_t ngraphs, uint32_t* __restrict__ Z) {
+  const unsigned lane = threadIdx.x & 31;
+  for (uint32_t g = blockIdx.x; g < ngraphs; g += gridDim.x) {
+    const RaggedGraph gr     = graphs[g];
+    const uint64_t    nwords = (gr.n + 31) / 32;
+    for (uint64_t w = threadIdx.x >> 5; w < nwords; w += blockDim.x >> 5) {
+      const uint64_t u    = w * 32 + lane;
+      const bool     zero = (u >= gr.n) || (off[gr.off_base + u + 1] == off[gr.off_base + u]);
+      const unsigned b    = __ballot_sync(kFullMask, zero);
+      if (lane == 0) Z[gr.z_base + w] = b;
+    }
+  }
 }
 
 int grid_for(const GraphDev* g, int per_sm) { return std::max(1, g->sm_count * per_sm); }
@@ -1295,6 +1420,65 @@ int component_edges(GraphDev* g, const uint32_t* parents, uint64_t* edges, uint6
 int widen_offsets(const uint32_t* src, uint64_t* dst, uint64_t count, cudaStream_t stream) {
   k_widen<<<592, kThreads, 0, stream>>>(src, dst, count);
   NWG_CUDA_TRY(cudaGetLastError());
+  return NWG_OK;
+}
+
+int ragged_slot_bytes(uint64_t nmax, uint64_t mmax, uint64_t* bytes) {
+  *bytes = slot_layout(nmax, mmax).bytes;
+  return NWG_OK;
+}
+
+int zero_indegree_packed(RaggedDev* r) {
+  if (r->ngraphs == 0) return NWG_OK;
+  k_zero_indegree_packed<<<std::max(1, r->sm_count * 4), kThreads>>>(r->off, r->graphs, r->ngraphs, r->Z);
+  NWG_CUDA_TRY(cudaGetLastError());
+  return NWG_OK;
+}
+
+// One persistent launch over the r->items table (already on the device),
+// captured into a CUDA graph with the counter reset and replayed while the
+// item count, slot count and output buffer stay the same.
+int ragged_launch(RaggedDev* r, uint32_t n_items, uint32_t* parents_dev, uint32_t blocks_per_sm, float* ms) {
+  const uint32_t slots = (uint32_t)std::max(1, r->sm_count * (int)blocks_per_sm);
+  if (!r->exec || r->exec_items != n_items || r->exec_slots != slots || r->exec_parents != parents_dev) {
+    if (r->exec) {
+      cudaGraphExecDestroy(r->exec);
+      r->exec = nullptr;
+    }
+    RaggedParams rp = {};
+    rp.off          = r->off;
+    rp.col          = r->col;
+    rp.Z            = r->Z;
+    rp.graphs       = r->graphs;
+    rp.items        = r->items;
+    rp.results      = r->results;
+    rp.parents      = parents_dev;
+    rp.n_items      = n_items;
+    rp.next_item    = r->counter;
+    rp.scratch      = r->scratch;
+    rp.slot_bytes   = slot_layout(r->nmax, r->mmax).bytes;
+    rp.nmax         = r->nmax;
+    rp.mmax         = r->mmax;
+    cudaGraph_t graph;
+    NWG_CUDA_TRY(cudaStreamBeginCapture(r->stream, cudaStreamCaptureModeThreadLocal));
+    cudaMemsetAsync(r->counter, 0, sizeof(unsigned int), r->stream);
+    k_ragged<<<slots, kThreads, 0, r->stream>>>(rp);
+    const cudaError_t le = cudaGetLastError();
+    const cudaError_t ce = cudaStreamEndCapture(r->stream, &graph);
+    if (le != cudaSuccess) return cuda_error(le, "k_ragged launch (capture)");
+    if (ce != cudaSuccess) return cuda_error(ce, "cudaStreamEndCapture(ragged)");
+    const cudaError_t ie = cudaGraphInstantiate(&r->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) return cuda_error(ie, "cudaGraphInstantiate(ragged)");
+    r->exec_items   = n_items;
+    r->exec_slots   = slots;
+    r->exec_parents = parents_dev;
+  }
+  NWG_CUDA_TRY(cudaEventRecord(r->ev0, r->stream));
+  NWG_CUDA_TRY(cudaGraphLaunch(r->exec, r->stream));
+  NWG_CUDA_TRY(cudaEventRecord(r->ev1, r->stream));
+  NWG_CUDA_TRY(cudaEventSynchronize(r->ev1));
+  if (ms) cudaEventElapsedTime(ms, r->ev0, r->ev1);
   return NWG_OK;
 }
 

@@ -157,6 +157,69 @@ struct MsWorkspace {
   cudaEvent_t  ev_lvl[2] = {nullptr, nullptr};
 };
 
+// Ragged batch (many small graphs, one persistent launch).
+struct RaggedGraph {  // one packed graph (device and host copies)
+  uint64_t n, m;
+  uint64_t off_base;  // index of the graph's first offset in the packed offsets
+  uint64_t col_base;  // index of its first column (a multiple of 4: 16-byte aligned)
+  uint64_t z_base;    // index of its first in-degree-zero bitmap word
+};
+
+struct RaggedItem {  // one (graph, root) traversal
+  uint32_t graph;
+  uint32_t root;
+  uint64_t out_base;  // index of the item's parents in the packed output
+  int32_t  alpha;
+  int32_t  beta;
+  uint32_t warp_min;  // degree threshold of the chunked queue
+  uint32_t pad;
+};
+
+struct RaggedResult {
+  int32_t  status;
+  uint32_t steps, levels, td_steps, bu_steps, b2q_steps;
+  uint64_t reached;
+};
+
+struct RaggedParams {
+  const uint64_t*     off;
+  const uint32_t*     col;
+  const uint32_t*     Z;
+  const RaggedGraph*  graphs;
+  const RaggedItem*   items;
+  RaggedResult*       results;
+  uint32_t*           parents;
+  uint32_t            n_items;
+  unsigned int*       next_item;
+  unsigned char*      scratch;  // one slot per resident block
+  uint64_t            slot_bytes;
+  uint64_t            nmax, mmax;
+};
+
+struct RaggedDev {
+  int                      device   = 0;
+  int                      sm_count = 148;
+  uint32_t                 ngraphs  = 0;
+  uint64_t                 nmax = 0, mmax = 0, total_n = 0;
+  uint64_t*                off      = nullptr;
+  uint32_t*                col      = nullptr;
+  uint32_t*                Z        = nullptr;
+  RaggedGraph*             graphs   = nullptr;
+  std::vector<RaggedGraph> graphs_host;
+  // run state (sized by the last run)
+  RaggedItem*              items    = nullptr;
+  RaggedResult*            results  = nullptr;
+  unsigned int*            counter  = nullptr;
+  unsigned char*           scratch  = nullptr;
+  uint64_t                 scratch_bytes = 0, items_cap = 0;
+  cudaStream_t             stream   = nullptr;
+  cudaEvent_t              ev0 = nullptr, ev1 = nullptr;
+  cudaGraphExec_t          exec     = nullptr;
+  uint32_t                 exec_items = 0, exec_slots = 0;
+  uint32_t*                exec_parents = nullptr;
+  std::mutex               mu;
+};
+
 struct GraphDev {
   int       device = 0;
   uint64_t  n = 0, m = 0, in_m = 0;
@@ -196,6 +259,10 @@ void fill_stats(const Ctrl& c, nwg_bfs_stats* s);
 int  build_zero_indegree(GraphDev* g, cudaStream_t stream);
 int  component_edges(GraphDev* g, const uint32_t* parents, uint64_t* edges, uint64_t* vertices);
 int  widen_offsets(const uint32_t* src, uint64_t* dst, uint64_t count, cudaStream_t stream);
+
+int  ragged_launch(RaggedDev* r, uint32_t n_items, uint32_t* parents_dev, uint32_t blocks_per_sm, float* ms);
+int  ragged_slot_bytes(uint64_t nmax, uint64_t mmax, uint64_t* bytes);
+int  zero_indegree_packed(RaggedDev* r);
 
 // nwg_msbfs.cu
 int  ms_ws_init(GraphDev* g, MsWorkspace* ws);
