@@ -52,6 +52,12 @@ GRAPH_SEED = 1
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum summed over the
+# kernels) of one traversal captured with ncu on a smaller graph of the same
+# kind, and that graph's directed entries; scaled to a workload by its
+# entries (profiles/dobfs_traffic_rmat22_uniform22.md).
+TRAFFIC_CAPTURES = {"rmat": (234.0e6, 128306546), "uniform": (542.8e6, 134217204)}
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -66,6 +72,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-ragged", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serve-slots", type=int, default=8)
     ap.add_argument("--profile-one", action="store_true",
                     help="after warm-up, run one traversal inside an NVTX range 'nwg_profile' and exit (for ncu)")
     return ap.parse_args()
@@ -331,6 +339,43 @@ def bench_ragged(nwg, torch, num_graphs=1000, reps=3):
             "classes": {k: v.__dict__ for k, v in params.items()}, "generate_s": gen_s, "autotune_s": tune_s}
 
 
+SERVE_RATES = (1000, 10000, 50000, 100000, 200000)
+
+
+def bench_serving(nwg, num_graphs=200, rates=SERVE_RATES, seconds=1.5, slots=8, budget=16 << 30):
+    """Serving: num_graphs resident graphs (the ragged distribution), an
+    open-loop Poisson stream of (graph, root) queries per offered rate
+    (`seconds` of arrivals, at least 2,000 queries), graph popularity
+    Zipf(1.1), per-query-state budget 16 GiB, same-graph queries coalesced
+    into multi-source passes, `slots` passes in flight.  Latency: scheduled
+    arrival to the answer (uint8 depth row) in pinned host memory."""
+    from nwgr_b200.serving import query_trace, serving_graphs
+
+    t0 = time.perf_counter()
+    graphs, pools = serving_graphs(nwg, num_graphs)
+    gen_s = time.perf_counter() - t0
+    csr_bytes = int(sum(8 * (g.n + 1) + 4 * g.m for g in graphs))
+    server = nwg.Server(graphs, slots=slots, budget_bytes=budget)
+    warm = query_trace(pools, 20000, 4000, seed=99)
+    server.run_trace(*warm)
+    out = []
+    for rate in rates:
+        count = int(max(2000, min(300000, rate * seconds)))
+        gid, roots, arr = query_trace(pools, rate, count, seed=int(rate) % 1000003)
+        _, bs, st = server.run_trace(gid, roots, arr)
+        out.append({"offered_qps": rate, "queries": count, "qps": st.qps, "p50_ms": st.p50_ms, "p99_ms": st.p99_ms,
+                    "max_ms": st.max_ms, "mean_batch": st.mean_batch, "batches": int(st.batches),
+                    "peak_in_flight": int(st.peak_in_flight),
+                    "overlap": st.batch_time_s / st.wall_s if st.wall_s > 0 else 0.0,
+                    "peak_state_bytes": int(st.peak_state_bytes), "answer_bytes": int(sum(graphs[g].n for g in gid))})
+    info = {"slots": int(st.slots), "slot_bytes": int(st.slot_bytes), "state_budget_bytes": int(st.budget_bytes)}
+    server.close()
+    for g in graphs:
+        g.release()
+    return {"graphs": num_graphs, "csr_bytes": csr_bytes, "zipf_s": 1.1, "budget_bytes": budget, **info,
+            "generate_s": gen_s, "rates": out}
+
+
 def cpu_baseline(off, cols, roots, n_roots):
     """Reference bfs.hpp on the host cores over a bounded sample of roots."""
     from oracle.oracle import Reference
@@ -446,7 +491,10 @@ def main():
     hbm, hbm_kind = peaks()
     b_r = 4.0 * e_r + 8.0 * n_r + 4.0 * n
     achieved_gbs = float(np.mean(b_r / (per_root_ms * 1e-3)) / 1e9)
-    traffic = os.environ.get("NWG_TRAFFIC_BYTES")
+    traffic = None
+    if spec["kind"] in TRAFFIC_CAPTURES:
+        cap_bytes, cap_m = TRAFFIC_CAPTURES[spec["kind"]]
+        traffic = cap_bytes * m / cap_m
 
     # e2e through the C ABI with host buffers
     e2e = None
@@ -486,6 +534,13 @@ def main():
             g.release()
             ws, g = None, None
         ragged = bench_ragged(nwg, torch)
+    serving = None
+    if not args.no_serving:
+        if ws is not None:
+            ws.close()
+            g.release()
+            ws, g = None, None
+        serving = bench_serving(nwg, slots=args.serve_slots)
     cpu = None
     if rank == 0 and not args.no_cpu:
         if g is None:
@@ -508,9 +563,12 @@ def main():
                          "frac": achieved_gbs / hbm, "peak_kind": hbm_kind,
                          "kernel": "one traversal (level-loop CUDA graph: k_init, k_decide, k_td, k_bu, k_b2q)",
                          "algorithmic_bytes_per_launch_mean": float(np.mean(b_r)),
-                         "traffic": float(traffic) if traffic else None},
+                         "traffic": traffic,
+                         "traffic_note": "ncu DRAM bytes of one traversal of the same graph kind at scale 22, "
+                                         "scaled by directed entries" if traffic else None},
             "gpu_launches": int(np.sum(launches)) * args.steps,
             "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, "batched": batched, "ragged": ragged,
+            "serving": serving,
         }
         print(json.dumps(line), flush=True)
     if ws is not None:

@@ -206,6 +206,57 @@ int nwg_ragged_bfs(nwg_ragged r, uint32_t num_items, const nwg_ragged_item* item
                    uint64_t* item_offsets_host, nwg_ragged_result* results_host, uint32_t blocks_per_sm,
                    float* device_ms);
 
+/* Serving: (graph, root) queries against registered graphs kept resident in
+ * HBM, answered as uint8 depth rows (depth per vertex, 255 = unreached; n
+ * bytes of the query's graph).  No reference counterpart: NWGraph answers
+ * one bfs call at a time; each answer equals the depths of that single-source
+ * BFS.  `slots` worker threads, each with its own CUDA stream and
+ * multi-source workspace, run batches concurrently: a free slot takes the
+ * graph of the oldest waiting query and coalesces up to max_batch waiting
+ * queries on that graph into one multi-source pass (nwg_msbfs).  Admission:
+ * a query taken by a slot holds 2.5 * n bytes of state (its device depth
+ * row, its pinned host row and one bit per vertex in four bitsets) until its
+ * answer is in host memory; taken state never exceeds the budget left after
+ * the slots' fixed buffers (max_batch 256 rows of the largest graph, device
+ * and pinned, plus the workspace), and queries that do not fit wait.  All
+ * graphs must live on one device and outlive the server. */
+typedef struct nwg_server_s* nwg_server;
+typedef struct {
+  uint32_t slots;        /* concurrent batches (0 = 8, at most 64; fewer if the budget holds fewer) */
+  uint32_t max_batch;    /* queries per multi-source pass (0 = 256, at most 256) */
+  uint64_t budget_bytes; /* slots' buffers + per-query state, device and pinned host (0 = 16 GiB) */
+  int32_t alpha;         /* push/pull switch of the multi-source pass (0 = 4) */
+} nwg_server_config;
+typedef struct {
+  uint64_t queries, batches, failed;
+  double wall_s;     /* first scheduled arrival to last answer */
+  double qps;        /* queries / wall_s */
+  double mean_batch; /* queries per multi-source pass */
+  double mean_ms, p50_ms, p99_ms, max_ms; /* latency: scheduled arrival to answer in host memory */
+  uint64_t peak_state_bytes; /* most per-query state held at once */
+  uint64_t budget_bytes;     /* per-query state budget left after the slots */
+  uint64_t slot_bytes;       /* fixed buffers of one slot */
+  uint32_t slots, peak_in_flight; /* slots created; most batches in flight at once */
+  double batch_time_s;       /* summed batch times (take to answer); / wall_s = mean overlap */
+} nwg_server_stats;
+int nwg_server_create(const nwg_graph* graphs, uint32_t num_graphs, const nwg_server_config* cfg, nwg_server* out);
+/* Stops the workers and frees the slots; no nwg_server_wait may be pending. */
+int nwg_server_destroy(nwg_server s);
+/* Queues one query; depths_host (n bytes of the graph, or NULL) receives the
+ * answer.  nwg_server_wait blocks until that query is answered and returns
+ * its status; latency_us = submit to answer. */
+int nwg_server_submit(nwg_server s, uint32_t graph, uint32_t root, uint8_t* depths_host, uint64_t* ticket);
+int nwg_server_wait(nwg_server s, uint64_t ticket, double* latency_us);
+/* Open-loop replay of a query trace: query i (graph[i], root[i]) is released
+ * at arrival_us[i] (non-decreasing, microseconds from the start) whatever
+ * the server's progress; returns when all are answered.  depths_host[i]
+ * (or the whole array) may be NULL; latency_us[i] and batch_size[i] (may be
+ * NULL) receive each query's latency from its scheduled arrival and the size
+ * of the pass that answered it. */
+int nwg_server_run_trace(nwg_server s, uint32_t count, const uint32_t* graph, const uint32_t* root,
+                         const double* arrival_us, uint8_t* const* depths_host, double* latency_us,
+                         uint32_t* batch_size, nwg_server_stats* stats);
+
 /* Direction-optimizing BFS that allocates no device memory.  No counterpart
  * in the reference: NWGraph's bfs allocates its state per call.  For callers
  * that may not call cudaMalloc/cudaFree (both synchronise the device; latency-

@@ -40,6 +40,7 @@ EXPORTED = (
     "nwg_bfs_topdown", "nwg_bfs_stepped", "nwg_component_edges", "nwg_graph_copy_csr", "nwg_gen_rmat", "nwg_gen_uniform",
     "nwg_gen_grid", "nwg_pick_roots", "nwg_bfs_noalloc", "nwg_msbfs_ws_create", "nwg_msbfs_ws_destroy",
     "nwg_msbfs", "nwg_ragged_register", "nwg_ragged_release", "nwg_ragged_info", "nwg_ragged_bfs",
+    "nwg_server_create", "nwg_server_destroy", "nwg_server_submit", "nwg_server_wait", "nwg_server_run_trace",
 )
 
 
@@ -105,6 +106,21 @@ class RaggedResult(C.Structure):
                 ("bu_steps", C.c_uint32), ("b2q_steps", C.c_uint32), ("reached", C.c_uint64)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("slots", C.c_uint32), ("max_batch", C.c_uint32), ("budget_bytes", C.c_uint64), ("alpha", C.c_int32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("queries", C.c_uint64), ("batches", C.c_uint64), ("failed", C.c_uint64), ("wall_s", C.c_double),
+                ("qps", C.c_double), ("mean_batch", C.c_double), ("mean_ms", C.c_double), ("p50_ms", C.c_double),
+                ("p99_ms", C.c_double), ("max_ms", C.c_double), ("peak_state_bytes", C.c_uint64),
+                ("budget_bytes", C.c_uint64), ("slot_bytes", C.c_uint64), ("slots", C.c_uint32),
+                ("peak_in_flight", C.c_uint32), ("batch_time_s", C.c_double)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 _vp = C.c_void_p
 _u32, _u64, _int = C.c_uint32, C.c_uint64, C.c_int
 
@@ -141,6 +157,11 @@ def _load():
         "nwg_ragged_release": (_int, [_vp]),
         "nwg_ragged_info": (_int, [_vp, C.POINTER(_u32), C.POINTER(_u64), C.POINTER(_u64), C.POINTER(_u64)]),
         "nwg_ragged_bfs": (_int, [_vp, _u32, _vp, _vp, _vp, _vp, _u32, C.POINTER(C.c_float)]),
+        "nwg_server_create": (_int, [_vp, _u32, C.POINTER(ServerConfig), C.POINTER(_vp)]),
+        "nwg_server_destroy": (_int, [_vp]),
+        "nwg_server_submit": (_int, [_vp, _u32, _u32, _vp, C.POINTER(_u64)]),
+        "nwg_server_wait": (_int, [_vp, _u64, C.POINTER(C.c_double)]),
+        "nwg_server_run_trace": (_int, [_vp, _u32, _vp, _vp, _vp, _vp, _vp, _vp, C.POINTER(ServerStats)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -355,6 +376,68 @@ class RaggedBatch:
         try:
             if self.h:
                 lib.nwg_ragged_release(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+class Server:
+    """Query server over resident graphs (nwg_server): (graph index, root)
+    queries answered as uint8 depth rows (255 = unreached), same-graph
+    queries coalesced into multi-source passes, `slots` batches in flight
+    at once, admission against `budget_bytes`."""
+
+    def __init__(self, graphs, slots: int = 8, max_batch: int = 256, budget_bytes: int = 16 << 30, alpha: int = 0):
+        self.graphs = list(graphs)  # kept alive: the server borrows them
+        hs = (_vp * len(self.graphs))(*[g.h for g in self.graphs])
+        cfg = ServerConfig(int(slots), int(max_batch), int(budget_bytes), int(alpha))
+        h = _vp()
+        check(lib.nwg_server_create(hs, len(self.graphs), C.byref(cfg), C.byref(h)))
+        self.h = h.value
+
+    def submit(self, graph: int, root: int, out: np.ndarray | None = None) -> int:
+        """Queues one query; `out` (uint8, n of the graph) receives the answer."""
+        if out is not None:
+            assert out.dtype == np.uint8 and out.flags.c_contiguous and out.size >= self.graphs[graph].n
+        t = _u64()
+        check(lib.nwg_server_submit(self.h, int(graph), int(root), None if out is None else out.ctypes.data,
+                                    C.byref(t)))
+        return t.value
+
+    def wait(self, ticket: int) -> float:
+        """Blocks until the query is answered; returns its latency in ms."""
+        lat = C.c_double()
+        check(lib.nwg_server_wait(self.h, int(ticket), C.byref(lat)))
+        return lat.value / 1e3
+
+    def run_trace(self, graph_ids, roots, arrival_us, outputs=None):
+        """Open-loop replay: query i released at arrival_us[i].  outputs: None
+        or a list of uint8 arrays (None entries allowed).  Returns (latency
+        ms per query, batch size per query, ServerStats)."""
+        g = np.ascontiguousarray(graph_ids, np.uint32)
+        r = np.ascontiguousarray(roots, np.uint32)
+        a = np.ascontiguousarray(arrival_us, np.float64)
+        k = g.size
+        assert r.size == k and a.size == k
+        outp = None
+        if outputs is not None:
+            outp = (C.c_void_p * k)(*[None if o is None else o.ctypes.data for o in outputs])
+        lat = np.zeros(k, np.float64)
+        bs = np.zeros(k, np.uint32)
+        st = ServerStats()
+        check(lib.nwg_server_run_trace(self.h, k, g.ctypes.data, r.ctypes.data, a.ctypes.data, outp,
+                                       lat.ctypes.data, bs.ctypes.data, C.byref(st)))
+        return lat / 1e3, bs, st
+
+    def close(self):
+        if self.h:
+            check(lib.nwg_server_destroy(self.h))
+            self.h = None
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib.nwg_server_destroy(self.h)
                 self.h = None
         except Exception:
             pass

@@ -141,15 +141,18 @@ struct Workspace {
 };
 
 // State of the batched multi-source BFS (nwg_msbfs.cu); sized for 256
-// sources (four 64-bit words) per vertex.
+// sources (four 64-bit words) per vertex of any graph with at most n_cap
+// vertices and m_cap out-edges.
 struct MsWorkspace {
-  GraphDev*    g       = nullptr;
+  GraphDev*    g       = nullptr;  // the graph it was created for (may be null for a shared one)
+  uint64_t     n_cap = 0, m_cap = 0;
   uint64_t*    vis     = nullptr;
   uint64_t*    fr[2]   = {nullptr, nullptr};
   uint64_t*    nx      = nullptr;
   uint64_t*    list[2] = {nullptr, nullptr};  // frontier chunk entries
   uint64_t     list_cap = 0;
   void*        cnt     = nullptr;
+  void*        cnt_host = nullptr;  // pinned mirror of the level counters
   uint32_t*    roots   = nullptr;
   uint32_t*    roots_uniq = nullptr;
   cudaStream_t stream  = nullptr;
@@ -265,8 +268,12 @@ int  ragged_slot_bytes(uint64_t nmax, uint64_t mmax, uint64_t* bytes);
 int  zero_indegree_packed(RaggedDev* r);
 
 // nwg_msbfs.cu
-int  ms_ws_init(GraphDev* g, MsWorkspace* ws);
-void ms_ws_free(MsWorkspace* ws);
+int      ms_ws_init(GraphDev* g, MsWorkspace* ws);
+int      ms_ws_init_cap(GraphDev* g, uint64_t n_cap, uint64_t m_cap, MsWorkspace* ws);
+uint64_t ms_ws_bytes(uint64_t n_cap, uint64_t m_cap);
+void     ms_ws_free(MsWorkspace* ws);
+int      ms_run_on(MsWorkspace* ws, GraphDev* g, const uint32_t* roots_host, uint32_t k, uint8_t* depths_dev, int alpha,
+                   cudaStream_t stream, nwg_msbfs_stats* st);
 int  ms_run(MsWorkspace* ws, const uint32_t* roots_host, uint32_t k, uint8_t* depths_dev, int alpha, cudaStream_t stream,
             nwg_msbfs_stats* st);
 

@@ -340,7 +340,13 @@ __global__ void k_ms_root_list(MsParams<W> p, const uint32_t* __restrict__ uniq,
   if (threadIdx.x == 0 && f) atomicAdd(&p.cnt->frontier_edges, f);
 }
 
-int grid_ms(const GraphDev* g, int per_sm) { return std::max(1, g->sm_count * per_sm); }
+// Grid of the grid-stride kernels: 8 blocks per SM, fewer when the graph
+// (or the frontier list) has less work than that, so the small graphs of a
+// serving mix leave room for other streams' launches.
+int grid_ms(const GraphDev* g, int per_sm, uint64_t items, uint64_t per_block) {
+  const uint64_t want = (items + per_block - 1) / per_block;
+  return (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)g->sm_count * per_sm, want));
+}
 
 // One pass of up to 64 * W sources.
 template <int W>
@@ -379,7 +385,7 @@ int ms_pass(GraphDev* g, MsWorkspace* ws, const uint32_t* roots_dev, const uint3
   std::sort(uniq.begin(), uniq.end());
   uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
   NWG_CUDA_TRY(cudaMemcpyAsync(ws->roots_uniq, uniq.data(), uniq.size() * 4, cudaMemcpyHostToDevice, stream));
-  MsCounters hc;
+  MsCounters& hc = *static_cast<MsCounters*>(ws->cnt_host);
   NWG_CUDA_TRY(cudaMemsetAsync(ws->cnt, 0, sizeof(MsCounters), stream));
   p.cnt = static_cast<MsCounters*>(ws->cnt);
   k_ms_root_list<W><<<1, kMsThreads, 0, stream>>>(p, ws->roots_uniq, (uint32_t)uniq.size());
@@ -399,13 +405,14 @@ int ms_pass(GraphDev* g, MsWorkspace* ws, const uint32_t* roots_dev, const uint3
     const bool traced = st->passes == 0 && st->trace_len < NWG_MS_TRACE_CAP;
     if (traced) NWG_CUDA_TRY(cudaEventRecord(ws->ev_lvl[0], stream));
     if (pull) {
-      k_ms_pull<W><<<grid_ms(g, 8), kMsThreads, 0, stream>>>(p);
+      k_ms_pull<W><<<grid_ms(g, 8, n, kMsThreads), kMsThreads, 0, stream>>>(p);
       st->pull_levels++;
     } else {
       unchecked -= std::min(unchecked, fedges);
-      k_ms_push<W><<<grid_ms(g, 8), kMsThreads, 0, stream>>>(p, std::min<uint64_t>(nlist, ws->list_cap));
+      const uint64_t nl = std::min<uint64_t>(nlist, ws->list_cap);
+      k_ms_push<W><<<grid_ms(g, 8, nl, kMsWarps), kMsThreads, 0, stream>>>(p, nl);
       NWG_CUDA_TRY(cudaGetLastError());
-      k_ms_finalize<W><<<grid_ms(g, 8), kMsThreads, 0, stream>>>(p);
+      k_ms_finalize<W><<<grid_ms(g, 8, n, kMsThreads), kMsThreads, 0, stream>>>(p);
       st->push_levels++;
     }
     NWG_CUDA_TRY(cudaGetLastError());
@@ -431,18 +438,27 @@ int ms_pass(GraphDev* g, MsWorkspace* ws, const uint32_t* roots_dev, const uint3
 
 }  // namespace
 
-int ms_ws_init(GraphDev* g, MsWorkspace* ws) {
-  const uint64_t n     = std::max<uint64_t>(g->n, 1);
-  const size_t   words = (size_t)n * 4 * sizeof(uint64_t);  // room for W = 4
-  // every frontier vertex has at most deg / kMsChunk + 1 entries
-  const uint64_t list_cap = n + g->m / kMsChunk + 1;
+uint64_t ms_ws_bytes(uint64_t n_cap, uint64_t m_cap) {
+  const uint64_t n = std::max<uint64_t>(n_cap, 1);
+  // VIS, FR[2], NX at four words per vertex, two frontier lists (every
+  // frontier vertex has at most deg / kMsChunk + 1 entries), counters, roots
+  return 4 * n * 4 * sizeof(uint64_t) + 2 * (n + m_cap / kMsChunk + 1) * 8 + sizeof(MsCounters) + 2 * 256 * 4;
+}
+
+int ms_ws_init_cap(GraphDev* g, uint64_t n_cap, uint64_t m_cap, MsWorkspace* ws) {
+  const uint64_t n        = std::max<uint64_t>(n_cap, 1);
+  const size_t   words    = (size_t)n * 4 * sizeof(uint64_t);  // room for W = 4
+  const uint64_t list_cap = n + m_cap / kMsChunk + 1;
   ws->g                   = g;
+  ws->n_cap               = n_cap;
+  ws->m_cap               = m_cap;
   ws->list_cap            = list_cap;
   if (cudaMalloc(&ws->vis, words) != cudaSuccess || cudaMalloc(&ws->fr[0], words) != cudaSuccess ||
       cudaMalloc(&ws->fr[1], words) != cudaSuccess || cudaMalloc(&ws->nx, words) != cudaSuccess ||
       cudaMalloc(&ws->list[0], list_cap * 8) != cudaSuccess || cudaMalloc(&ws->list[1], list_cap * 8) != cudaSuccess ||
       cudaMalloc(&ws->cnt, sizeof(MsCounters)) != cudaSuccess || cudaMalloc(&ws->roots, 256 * 4) != cudaSuccess ||
-      cudaMalloc(&ws->roots_uniq, 256 * 4) != cudaSuccess) {
+      cudaMalloc(&ws->roots_uniq, 256 * 4) != cudaSuccess ||
+      cudaMallocHost(&ws->cnt_host, sizeof(MsCounters)) != cudaSuccess) {
     cudaGetLastError();
     return set_error(NWG_ENOMEM, "multi-source workspace allocation failed");
   }
@@ -453,6 +469,8 @@ int ms_ws_init(GraphDev* g, MsWorkspace* ws) {
   NWG_CUDA_TRY(cudaEventCreate(&ws->ev_lvl[1]));
   return NWG_OK;
 }
+
+int ms_ws_init(GraphDev* g, MsWorkspace* ws) { return ms_ws_init_cap(g, g->n, g->m, ws); }
 
 void ms_ws_free(MsWorkspace* ws) {
   if (!ws) return;
@@ -466,6 +484,7 @@ void ms_ws_free(MsWorkspace* ws) {
   cudaFree(ws->cnt);
   cudaFree(ws->roots);
   cudaFree(ws->roots_uniq);
+  if (ws->cnt_host) cudaFreeHost(ws->cnt_host);
   if (ws->ev0) cudaEventDestroy(ws->ev0);
   if (ws->ev1) cudaEventDestroy(ws->ev1);
   if (ws->ev_lvl[0]) cudaEventDestroy(ws->ev_lvl[0]);
@@ -474,10 +493,12 @@ void ms_ws_free(MsWorkspace* ws) {
   delete ws;
 }
 
-// Runs ceil(k / 256) passes of up to 256 sources on ws->stream (or `stream`).
-int ms_run(MsWorkspace* ws, const uint32_t* roots_host, uint32_t k, uint8_t* depths_dev, int alpha,
-           cudaStream_t stream, nwg_msbfs_stats* st) {
-  GraphDev* g = ws->g;
+// Runs ceil(k / 256) passes of up to 256 sources over graph g, which must
+// fit the workspace's capacity, on `stream` (or the workspace's own).
+int ms_run_on(MsWorkspace* ws, GraphDev* g, const uint32_t* roots_host, uint32_t k, uint8_t* depths_dev, int alpha,
+              cudaStream_t stream, nwg_msbfs_stats* st) {
+  if (g->n > ws->n_cap || g->m > ws->m_cap)
+    return set_error(NWG_EINVAL, "graph larger than the multi-source workspace's capacity");
   for (uint32_t i = 0; i < k; ++i)
     if (roots_host[i] >= g->n) return set_error(NWG_EINVAL, "root " + std::to_string(roots_host[i]) + " >= n");
   if (alpha <= 0) return set_error(NWG_EINVAL, "alpha must be positive");
@@ -500,6 +521,11 @@ int ms_run(MsWorkspace* ws, const uint32_t* roots_host, uint32_t k, uint8_t* dep
     st->passes++;
   }
   return NWG_OK;
+}
+
+int ms_run(MsWorkspace* ws, const uint32_t* roots_host, uint32_t k, uint8_t* depths_dev, int alpha,
+           cudaStream_t stream, nwg_msbfs_stats* st) {
+  return ms_run_on(ws, ws->g, roots_host, k, depths_dev, alpha, stream, st);
 }
 
 }  // namespace nwg

@@ -42,6 +42,11 @@ def test_version_and_error_paths_without_gpu(nwg):
     assert nwg.lib.nwg_gen_rmat(10, 16, 1, 5, 2, 3, C.byref(C.c_void_p())) == nwg.NWG_EINVAL
     # the no-allocation entry point refuses out-of-limit sizes before touching the device
     assert nwg.lib.nwg_bfs_noalloc(None, None, None, None, 10, 0, 15, 18, None, None) == nwg.NWG_EINVAL
+    # the server refuses an empty graph set and unknown handles without a device
+    h = C.c_void_p()
+    assert nwg.lib.nwg_server_create(None, 0, None, C.byref(h)) == nwg.NWG_EINVAL and not h.value
+    assert nwg.lib.nwg_server_destroy(None) == nwg.NWG_EINVAL
+    assert nwg.lib.nwg_server_run_trace(None, 0, None, None, None, None, None, None, None) == nwg.NWG_EINVAL
     buf = C.create_string_buffer(8)
     length = nwg.lib.nwg_last_error(buf, 8)
     assert length > 7 and len(buf.value) == 7  # truncated, NUL-terminated

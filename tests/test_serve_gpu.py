@@ -1,0 +1,128 @@
+"""Serving loop (nwg_server): each query's answer is the same alone and in
+the mix.
+
+An answer is the uint8 depth row of one (graph, root) single-source BFS
+(255 = unreached), bit-exact against the oracle's serial BFS.  "Alone": a
+server with one slot and batches of one, each query submitted and awaited
+by itself.  "In the mix": the same queries replayed as a burst and as a
+Poisson stream through a server with several slots, so queries are
+coalesced into multi-source passes with other queries (same graph,
+different roots, duplicates included) while other passes run on other
+streams.  The tolerance is zero: depths are integers.
+"""
+import numpy as np
+import pytest
+
+from oracle import graphgen as gg
+
+pytestmark = pytest.mark.gpu
+
+NULL = 0xFFFFFFFF
+
+
+def _u8(d):
+    return np.where(d == NULL, 255, d).astype(np.uint8)
+
+
+@pytest.fixture(scope="module")
+def served(nwg):
+    rng = np.random.default_rng(4)
+    host = [gg.rmat(10, 16, seed=1), gg.rmat(12, 8, seed=2), gg.rmat(13, 24, seed=3), gg.grid(40, 30, 1, seed=4),
+            gg.grid(64, 64, 1, seed=5), gg.uniform(3000, 12, seed=6)]
+    # a directed graph (pull passes read the in-CSR)
+    n = 2500
+    u = rng.integers(0, n, 20000).astype(np.uint64)
+    v = rng.integers(0, n, 20000).astype(np.uint64)
+    doff, dcols = gg.directed_csr(u, v, n)
+    host.append((doff, dcols) + gg.transpose(doff, dcols, n))
+    graphs = [nwg.Graph.from_csr(*h) for h in host]
+    pools = [gg.roots(h[0], 8, seed=i + 1) for i, h in enumerate(host)]
+    yield host, graphs, pools
+    for g in graphs:
+        g.release()
+
+
+def _queries(pools, count, seed):
+    rng = np.random.default_rng(seed)
+    gid = rng.integers(0, len(pools), count).astype(np.uint32)
+    roots = np.array([pools[g][rng.integers(0, pools[g].size)] for g in gid], np.uint32)
+    return gid, roots
+
+
+def test_each_answer_same_alone_and_in_the_mix(nwg, port, served):
+    host, graphs, pools = served
+    gid, roots = _queries(pools, 400, seed=9)
+    want = {}
+    for g, r in set(zip(gid.tolist(), roots.tolist())):
+        h = host[g]
+        want[(g, r)] = _u8(port.depths(h[0], h[1], r))
+
+    alone = nwg.Server(graphs, slots=1, max_batch=1)
+    alone_out = []
+    for g, r in zip(gid.tolist(), roots.tolist()):
+        out = np.full(graphs[g].n, 7, np.uint8)
+        alone.wait(alone.submit(g, r, out))
+        assert np.array_equal(out, want[(g, r)]), f"alone: graph {g} root {r}"
+        alone_out.append(out)
+    alone.close()
+
+    mix = nwg.Server(graphs, slots=4, max_batch=256)
+    burst = np.zeros(gid.size)  # everything at once: the largest batches
+    poisson = np.cumsum(np.random.default_rng(3).exponential(1e6 / 20000.0, gid.size))
+    for arrival in (burst, poisson):
+        outs = [np.full(graphs[g].n, 7, np.uint8) for g in gid]
+        lat, bs, st = mix.run_trace(gid, roots, arrival, outs)
+        assert st.failed == 0 and st.queries == gid.size
+        for i, (g, r) in enumerate(zip(gid.tolist(), roots.tolist())):
+            assert np.array_equal(outs[i], alone_out[i]), f"query {i}: graph {g} root {r} differs in the mix"
+        assert np.all(lat > 0) and np.all(bs >= 1)
+        assert st.p50_ms <= st.p99_ms <= st.max_ms
+        assert st.batches >= 1 and abs(st.mean_batch - gid.size / st.batches) < 1e-9
+    # the burst was coalesced and ran on several slots at once
+    lat, bs, st = mix.run_trace(gid, roots, burst)
+    assert bs.max() > 1 and st.mean_batch > 1.0
+    assert st.peak_in_flight >= 2
+    mix.close()
+
+
+def test_admission_budget_bounds_state(nwg, served):
+    host, graphs, pools = served
+    gid, roots = _queries(pools, 300, seed=12)
+    big = max(g.n for g in graphs)
+    probe = nwg.Server(graphs, slots=1, budget_bytes=1 << 34)
+    slot_bytes = probe.run_trace(gid[:1], roots[:1], [0.0])[2].slot_bytes
+    probe.close()
+    # two slots plus room for only a handful of queries: most wait for budget
+    budget = 2 * slot_bytes + 8 * int(2.5 * big) + 4096
+    s = nwg.Server(graphs, slots=2, budget_bytes=budget)
+    outs = [np.zeros(graphs[g].n, np.uint8) for g in gid]
+    lat, bs, st = s.run_trace(gid, roots, np.zeros(gid.size), outs)
+    assert st.slots == 2 and st.failed == 0
+    assert st.peak_state_bytes <= st.budget_bytes
+    # a pass holds queries of one graph: the budget, not max_batch, bounded it
+    qbytes = np.array([2 * graphs[g].n + (4 * graphs[g].n + 7) // 8 for g in gid], np.int64)
+    assert np.all(bs.astype(np.int64) * qbytes <= st.budget_bytes)
+    assert bs.max() < 256
+    ref = nwg.Server(graphs, slots=1)
+    for i in range(0, gid.size, 37):
+        out = np.zeros(graphs[gid[i]].n, np.uint8)
+        ref.wait(ref.submit(int(gid[i]), int(roots[i]), out))
+        assert np.array_equal(out, outs[i])
+    ref.close()
+    s.close()
+
+
+def test_server_argument_errors(nwg, served):
+    _, graphs, _ = served
+    s = nwg.Server(graphs, slots=1)
+    with pytest.raises(nwg.NwgError) as e:
+        s.submit(len(graphs), 0)
+    assert e.value.code == nwg.NWG_EINVAL
+    with pytest.raises(nwg.NwgError):
+        s.submit(0, graphs[0].n)
+    with pytest.raises(nwg.NwgError):
+        s.run_trace([0, 0], [1, 2], [5.0, 1.0])  # arrivals must not decrease
+    s.close()
+    with pytest.raises(nwg.NwgError) as e:
+        nwg.Server(graphs, budget_bytes=1 << 20)  # no slot fits
+    assert "budget" in str(e.value)
