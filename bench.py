@@ -73,7 +73,7 @@ def parse():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-ragged", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
-    ap.add_argument("--serve-slots", type=int, default=8)
+    ap.add_argument("--serve-slots", type=int, default=16)
     ap.add_argument("--profile-one", action="store_true",
                     help="after warm-up, run one traversal inside an NVTX range 'nwg_profile' and exit (for ncu)")
     return ap.parse_args()
@@ -342,7 +342,7 @@ def bench_ragged(nwg, torch, num_graphs=1000, reps=3):
 SERVE_RATES = (1000, 10000, 50000, 100000, 200000)
 
 
-def bench_serving(nwg, num_graphs=200, rates=SERVE_RATES, seconds=1.5, slots=8, budget=16 << 30):
+def bench_serving(nwg, num_graphs=200, rates=SERVE_RATES, seconds=1.5, slots=16, budget=16 << 30):
     """Serving: num_graphs resident graphs (the ragged distribution), an
     open-loop Poisson stream of (graph, root) queries per offered rate
     (`seconds` of arrivals, at least 2,000 queries), graph popularity

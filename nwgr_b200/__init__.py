@@ -387,7 +387,7 @@ class Server:
     queries coalesced into multi-source passes, `slots` batches in flight
     at once, admission against `budget_bytes`."""
 
-    def __init__(self, graphs, slots: int = 8, max_batch: int = 256, budget_bytes: int = 16 << 30, alpha: int = 0):
+    def __init__(self, graphs, slots: int = 16, max_batch: int = 256, budget_bytes: int = 16 << 30, alpha: int = 0):
         self.graphs = list(graphs)  # kept alive: the server borrows them
         hs = (_vp * len(self.graphs))(*[g.h for g in self.graphs])
         cfg = ServerConfig(int(slots), int(max_batch), int(budget_bytes), int(alpha))

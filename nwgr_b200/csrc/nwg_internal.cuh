@@ -144,20 +144,22 @@ struct Workspace {
 // sources (four 64-bit words) per vertex of any graph with at most n_cap
 // vertices and m_cap out-edges.
 struct MsWorkspace {
-  GraphDev*    g       = nullptr;  // the graph it was created for (may be null for a shared one)
-  uint64_t     n_cap = 0, m_cap = 0;
-  uint64_t*    vis     = nullptr;
-  uint64_t*    fr[2]   = {nullptr, nullptr};
-  uint64_t*    nx      = nullptr;
-  uint64_t*    list[2] = {nullptr, nullptr};  // frontier chunk entries
-  uint64_t     list_cap = 0;
-  void*        cnt     = nullptr;
-  void*        cnt_host = nullptr;  // pinned mirror of the level counters
-  uint32_t*    roots   = nullptr;
-  uint32_t*    roots_uniq = nullptr;
-  cudaStream_t stream  = nullptr;
-  cudaEvent_t  ev0 = nullptr, ev1 = nullptr;
-  cudaEvent_t  ev_lvl[2] = {nullptr, nullptr};
+  GraphDev*       g       = nullptr;  // the graph it was created for (may be null for a shared one)
+  uint64_t        n_cap = 0, m_cap = 0;
+  int             sm_count = 148;
+  uint64_t*       vis     = nullptr;
+  uint64_t*       fr[2]   = {nullptr, nullptr};
+  uint64_t*       nx      = nullptr;
+  uint64_t*       list[2] = {nullptr, nullptr};  // frontier chunk entries
+  uint64_t        list_cap = 0;
+  void*           pass_dev  = nullptr;  // arguments and level-loop state of a pass (device)
+  void*           pass_host = nullptr;  // pinned staging of the same record
+  cudaGraphExec_t exec[4] = {nullptr, nullptr, nullptr, nullptr};  // pass graphs, one per word count W
+  cudaGraph_t     tmpl[4] = {nullptr, nullptr, nullptr, nullptr};  // their templates (own the nodes below)
+  cudaGraphNode_t nodes[4][8] = {};                                // kernel nodes updated per pass
+  bool            stepped = false;      // host-driven levels (NWG_MS_STEPPED=1), for profilers
+  cudaStream_t    stream  = nullptr;
+  cudaEvent_t     ev0 = nullptr, ev1 = nullptr;
 };
 
 // Ragged batch (many small graphs, one persistent launch).

@@ -19,6 +19,8 @@
 // chosen like the single-source switch: pull when the frontier's out-edges
 // exceed the unexplored edges / alpha (nw::graph::bfs, bfs.hpp:186).
 #include <algorithm>
+#include <cstdlib>
+#include <cstring>
 #include <vector>
 
 #include "nwg_internal.cuh"
@@ -41,25 +43,48 @@ constexpr uint32_t kMsChunk      = 256;  // out-edges per frontier chunk entry (
 constexpr uint32_t kMsChunkShift = 8;
 constexpr uint64_t kMsLaneChunks = 16;  // a lane writes up to this many chunk entries of one vertex itself
 
+// Level-loop state of a pass in device memory: the decide kernel advances
+// it, the level kernels read the level number and list length from it.
+constexpr uint32_t kMsTrace = NWG_MS_TRACE_CAP;
+struct MsPassDev {
+  uint64_t   list_cap;
+  uint32_t   k, nuniq;
+  int32_t    alpha;
+  uint32_t   level;      // level being run (0 = roots)
+  uint64_t   unchecked;  // out-edges not yet pushed (the switch's edges_to_check)
+  uint64_t   nlist;      // chunk entries of the current frontier list
+  int32_t    status;
+  uint32_t   levels;     // max depth + 1
+  uint32_t   pull, stopped, push_levels, pull_levels, trace_len;
+  MsCounters cnt[2];     // level L's kernels add into cnt[L & 1]
+  uint32_t   roots[256], uniq[256];
+  uint8_t    tr_pull[kMsTrace];
+  uint64_t   tr_fedges[kMsTrace], tr_disc[kMsTrace], tr_t[kMsTrace + 1];
+};
+
+// Kernel arguments (constant bank).  Level L reads FR[(L-1)&1] and
+// list[(L-1)&1] and writes FR[L&1], list[L&1], cnt[L&1]; the pass graph
+// holds one set of level nodes per parity, so these pointers are fixed per
+// node.  The roots are level 0 (FR[0], list[0], cnt[0]).
 template <int W>
 struct MsParams {
-  const uint64_t* off;
-  const uint32_t* col;
-  const uint64_t* in_off;
-  const uint32_t* in_col;
-  const uint32_t* Z;  // vertices with no in-edges: never reached by a pull
-  uint64_t        n;
-  uint64_t*       vis;
-  uint64_t*       fr_cur;
-  uint64_t*       fr_nxt;
-  uint64_t*       nx;
-  uint64_t*       list_cur;  // frontier chunk entries (vertex << 32 | chunk), push input
-  uint64_t*       list_nxt;
-  uint64_t        list_cap;
-  uint8_t*        depth;     // [k][n], rows of this pass start at depth + src0 * n
-  uint64_t        full[W];   // mask of the valid sources of each word
-  uint32_t        level;
-  MsCounters*     cnt;       // counters of the level being produced
+  const uint64_t*  off;
+  const uint32_t*  col;
+  const uint64_t*  in_off;
+  const uint32_t*  in_col;
+  const uint32_t*  Z;  // vertices with no in-edges: never reached by a pull
+  uint64_t         n;
+  uint64_t*        vis;
+  uint64_t*        fr_cur;
+  uint64_t*        fr_nxt;
+  uint64_t*        nx;
+  uint64_t*        list_cur;  // frontier chunk entries (vertex << 32 | chunk), push input
+  uint64_t*        list_nxt;
+  uint64_t         list_cap;
+  uint8_t*         depth;     // [k][n], rows of this pass start at depth + src0 * n
+  uint64_t         full[W];   // mask of the valid sources of each word
+  MsCounters*      cnt;       // counters of the level being produced
+  const MsPassDev* d;
 };
 
 template <typename T>
@@ -84,7 +109,8 @@ __device__ __forceinline__ T ms_block_sum(T v) {
 // consecutive vertices; the warp walks only the bits some lane has, so each
 // store instruction writes one row's bytes for up to 32 adjacent vertices.
 template <int W>
-__device__ __forceinline__ void write_depths(const MsParams<W>& p, bool has, uint64_t v, const uint64_t (&nw)[W]) {
+__device__ __forceinline__ void write_depths(const MsParams<W>& p, uint32_t level, bool has, uint64_t v,
+                                             const uint64_t (&nw)[W]) {
 #pragma unroll
   for (int w = 0; w < W; ++w) {
     uint64_t any = has ? nw[w] : 0ull;
@@ -93,7 +119,7 @@ __device__ __forceinline__ void write_depths(const MsParams<W>& p, bool has, uin
     while (any) {
       const int s = __ffsll((long long)any) - 1;
       any &= any - 1;
-      if (has && ((nw[w] >> s) & 1ull)) p.depth[(uint64_t)(w * 64 + s) * p.n + v] = (uint8_t)p.level;
+      if (has && ((nw[w] >> s) & 1ull)) p.depth[(uint64_t)(w * 64 + s) * p.n + v] = (uint8_t)level;
     }
   }
 }
@@ -101,20 +127,21 @@ __device__ __forceinline__ void write_depths(const MsParams<W>& p, bool has, uin
 // Roots: VIS, FR[cur] and depth 0 for each source; the frontier list holds
 // the distinct roots (deduplicated on the host).
 template <int W>
-__global__ void k_ms_roots(MsParams<W> p, const uint32_t* roots, uint32_t k) {
+__global__ void k_ms_roots(MsParams<W> p) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= k) return;
-  const uint64_t v   = roots[s];
+  if (s >= p.d->k) return;
+  const uint64_t v   = p.d->roots[s];
   const uint64_t bit = 1ull << (s & 63);
   atomicOr((unsigned long long*)&p.vis[v * W + (s >> 6)], (unsigned long long)bit);
-  atomicOr((unsigned long long*)&p.fr_cur[v * W + (s >> 6)], (unsigned long long)bit);
+  atomicOr((unsigned long long*)&p.fr_nxt[v * W + (s >> 6)], (unsigned long long)bit);
   p.depth[(uint64_t)s * p.n + v] = 0;
 }
 
 // Push: one warp per frontier chunk entry (up to kMsChunk out-edges of one
 // vertex), so hubs are spread over the grid; lanes stride over the edges.
 template <int W>
-__global__ void __launch_bounds__(kMsThreads) k_ms_push(MsParams<W> p, uint64_t nlist) {
+__global__ void __launch_bounds__(kMsThreads) k_ms_push(MsParams<W> p) {
+  const uint64_t nlist = p.d->nlist;
   const unsigned lane   = threadIdx.x & 31;
   const uint64_t gwarp  = (uint64_t)blockIdx.x * kMsWarps + (threadIdx.x >> 5);
   const uint64_t nwarps = (uint64_t)gridDim.x * kMsWarps;
@@ -178,6 +205,7 @@ __device__ __forceinline__ void ms_append(const MsParams<W>& p, bool has, uint32
 // Every vertex's FR[nxt] words are written (zero when nothing is new).
 template <int W>
 __global__ void __launch_bounds__(kMsThreads) k_ms_finalize(MsParams<W> p) {
+  const uint32_t level = p.d->level;
   unsigned long long disc = 0, fedges = 0;
   const uint64_t     stride = (uint64_t)gridDim.x * blockDim.x;
   const uint64_t     n_up   = (p.n + 31) & ~31ull;
@@ -201,13 +229,13 @@ __global__ void __launch_bounds__(kMsThreads) k_ms_finalize(MsParams<W> p) {
         disc += __popcll(nw[w]);
       }
     }
-    write_depths<W>(p, has, v, nw);
+    write_depths<W>(p, level, has, v, nw);
     ms_append<W>(p, has, (uint32_t)v, fedges, has ? (unsigned long long)(p.off[v + 1] - p.off[v]) : 0ull);
   }
-  const unsigned long long d = ms_block_sum(disc);
-  const unsigned long long f = ms_block_sum(fedges);
+  const unsigned long long dsum = ms_block_sum(disc);
+  const unsigned long long f    = ms_block_sum(fedges);
   if (threadIdx.x == 0) {
-    if (d) atomicAdd(&p.cnt->discovered, d);
+    if (dsum) atomicAdd(&p.cnt->discovered, dsum);
     if (f) atomicAdd(&p.cnt->frontier_edges, f);
   }
 }
@@ -217,6 +245,7 @@ __global__ void __launch_bounds__(kMsThreads) k_ms_finalize(MsParams<W> p) {
 // longer than kMsLaneDeg are scanned by the whole warp afterwards.
 template <int W>
 __global__ void __launch_bounds__(kMsThreads) k_ms_pull(MsParams<W> p) {
+  const uint32_t level = p.d->level;
   const unsigned     lane   = threadIdx.x & 31;
   unsigned long long disc = 0, fedges = 0;
   const uint64_t     stride = (uint64_t)gridDim.x * blockDim.x;
@@ -314,13 +343,13 @@ __global__ void __launch_bounds__(kMsThreads) k_ms_pull(MsParams<W> p) {
       has |= nw[w] != 0;
       disc += __popcll(nw[w]);
     }
-    write_depths<W>(p, has, v, nw);
+    write_depths<W>(p, level, has, v, nw);
     ms_append<W>(p, has, (uint32_t)v, fedges, has ? (unsigned long long)(p.off[v + 1] - p.off[v]) : 0ull);
   }
-  const unsigned long long d = ms_block_sum(disc);
-  const unsigned long long f = ms_block_sum(fedges);
+  const unsigned long long dsum = ms_block_sum(disc);
+  const unsigned long long f    = ms_block_sum(fedges);
   if (threadIdx.x == 0) {
-    if (d) atomicAdd(&p.cnt->discovered, d);
+    if (dsum) atomicAdd(&p.cnt->discovered, dsum);
     if (f) atomicAdd(&p.cnt->frontier_edges, f);
   }
 }
@@ -328,7 +357,9 @@ __global__ void __launch_bounds__(kMsThreads) k_ms_pull(MsParams<W> p) {
 // The first frontier list (chunk entries of the distinct roots) and its
 // out-edge count.  One block; every thread of it calls ms_append.
 template <int W>
-__global__ void k_ms_root_list(MsParams<W> p, const uint32_t* __restrict__ uniq, uint32_t nuniq) {
+__global__ void k_ms_root_list(MsParams<W> p) {  // level 0: writes list[0] and cnt[0]
+  const uint32_t*    uniq   = p.d->uniq;
+  const uint32_t     nuniq  = p.d->nuniq;
   unsigned long long fedges = 0;
   for (uint32_t base = 0; base < nuniq; base += blockDim.x) {
     const uint32_t i   = base + threadIdx.x;
@@ -340,98 +371,322 @@ __global__ void k_ms_root_list(MsParams<W> p, const uint32_t* __restrict__ uniq,
   if (threadIdx.x == 0 && f) atomicAdd(&p.cnt->frontier_edges, f);
 }
 
-// Grid of the grid-stride kernels: 8 blocks per SM, fewer when the graph
-// (or the frontier list) has less work than that, so the small graphs of a
-// serving mix leave room for other streams' launches.
-int grid_ms(const GraphDev* g, int per_sm, uint64_t items, uint64_t per_block) {
-  const uint64_t want = (items + per_block - 1) / per_block;
-  return (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)g->sm_count * per_sm, want));
+// The level loop's decision, one thread, before every level: stop when the
+// level just run discovered nothing (or a depth would reach 255), else pull
+// when the frontier's out-edges exceed the unpushed edges / alpha
+// (nw::graph::bfs, bfs.hpp:186), push otherwise.  Records the per-level
+// trace; with set_cond it drives the graph's WHILE node and this parity's
+// SWITCH node.  Once stopped, later calls only keep the loop stopped.
+__global__ void k_ms_decide(MsPassDev* d, cudaGraphConditionalHandle h_loop, cudaGraphConditionalHandle h_sw,
+                            int set_cond) {
+  if (threadIdx.x != 0) return;
+  bool stop = d->stopped != 0;
+  if (!stop) {
+    const uint32_t    L    = d->level + 1;
+    const MsCounters& prev = d->cnt[(L - 1) & 1];
+    uint64_t          now;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+    if (L - 1 <= kMsTrace) d->tr_t[L - 1] = now;
+    if (L > 1) {
+      if (L - 2 < kMsTrace) d->tr_disc[L - 2] = prev.discovered;
+      if (prev.discovered == 0) stop = true;
+      else d->levels = L;
+    }
+    if (!stop && L >= 255) {
+      d->status = NWG_EOVERFLOW;
+      stop      = true;
+    }
+    if (stop) {
+      d->trace_len = min(L - 1, kMsTrace);
+      d->stopped   = 1;
+    } else {
+      const uint64_t fedges = prev.frontier_edges;
+      d->nlist              = min((uint64_t)prev.frontier_count, d->list_cap);
+      d->cnt[L & 1]         = MsCounters{0, 0, 0};
+      const bool pull       = fedges > d->unchecked / (uint64_t)d->alpha;
+      if (!pull) d->unchecked -= min(d->unchecked, fedges);
+      if (L - 1 < kMsTrace) {
+        d->tr_pull[L - 1]   = pull ? 1 : 0;
+        d->tr_fedges[L - 1] = fedges;
+      }
+      if (pull) d->pull_levels++;
+      else d->push_levels++;
+      d->pull  = pull ? 1 : 0;
+      d->level = L;
+    }
+  }
+  if (set_cond) {
+    cudaGraphSetConditional(h_sw, stop ? 2u : d->pull);
+    cudaGraphSetConditional(h_loop, stop ? 0u : 1u);
+  }
 }
 
-// One pass of up to 64 * W sources.
+// Grids of the grid-stride kernels: 8 blocks per SM, fewer when the largest
+// graph the workspace takes has less work than that, so the small graphs of
+// a serving mix leave room for other streams' launches.
+int grid_ms(const MsWorkspace* ws, uint64_t items, uint64_t per_block) {
+  const uint64_t want = (items + per_block - 1) / per_block;
+  return (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)ws->sm_count * 8, want));
+}
+
+// Node slots of a pass graph.
+enum { kNRoots, kNList, kNPush0, kNFin0, kNPull0, kNPush1, kNFin1, kNPull1, kNNodes };
+
+// Arguments of a pass: the base set (roots, level 0) and the two parities.
 template <int W>
-int ms_pass(GraphDev* g, MsWorkspace* ws, const uint32_t* roots_dev, const uint32_t* roots_host, uint32_t k,
-            uint8_t* depth_rows, int alpha, cudaStream_t stream, nwg_msbfs_stats* st) {
-  const uint64_t n = g->n;
-  MsParams<W>    p = {};
-  p.off            = g->off;
-  p.col            = g->col;
-  p.in_off         = g->in_off;
-  p.in_col         = g->in_col;
-  p.Z              = g->Z;
-  p.n              = n;
-  p.vis            = ws->vis;
-  p.fr_cur         = ws->fr[0];
-  p.fr_nxt         = ws->fr[1];
-  p.nx             = ws->nx;
-  p.list_cur       = ws->list[0];
-  p.list_nxt       = ws->list[1];
-  p.list_cap       = ws->list_cap;
-  p.depth          = depth_rows;
+struct MsArgs {
+  MsParams<W> base;    // level 0: writes FR[0], list[0], cnt[0]
+  MsParams<W> par[2];  // par[L & 1] for level L
+};
+
+template <int W>
+MsArgs<W> ms_args(GraphDev* g, MsWorkspace* ws, uint8_t* depth_rows, uint32_t k) {
+  MsArgs<W>    a;
+  MsParams<W>& p = a.base;
+  std::memset(&p, 0, sizeof p);
+  p.off      = g->off;
+  p.col      = g->col;
+  p.in_off   = g->in_off;
+  p.in_col   = g->in_col;
+  p.Z        = g->Z;
+  p.n        = g->n;
+  p.vis      = ws->vis;
+  p.nx       = ws->nx;
+  p.list_cap = ws->list_cap;
+  p.depth    = depth_rows;
   for (int w = 0; w < W; ++w) {
     const int64_t bits = std::min<int64_t>(64, (int64_t)k - 64 * w);
     p.full[w]          = bits >= 64 ? ~0ull : bits <= 0 ? 0ull : ((1ull << bits) - 1);
   }
+  MsPassDev* d = static_cast<MsPassDev*>(ws->pass_dev);
+  p.d          = d;
+  for (int par = 0; par < 2; ++par) {  // level L with L & 1 == par
+    MsParams<W>& q = a.par[par];
+    q              = p;
+    q.fr_cur       = ws->fr[par ^ 1];
+    q.fr_nxt       = ws->fr[par];
+    q.list_cur     = ws->list[par ^ 1];
+    q.list_nxt     = ws->list[par];
+    q.cnt          = &d->cnt[par];
+  }
+  p.fr_nxt   = ws->fr[0];
+  p.list_nxt = ws->list[0];
+  p.cnt      = &d->cnt[0];
+  return a;
+}
+
+template <int W>
+void* ms_node_fn(int slot) {
+  switch (slot) {
+    case kNRoots: return (void*)k_ms_roots<W>;
+    case kNList: return (void*)k_ms_root_list<W>;
+    case kNPush0:
+    case kNPush1: return (void*)k_ms_push<W>;
+    case kNFin0:
+    case kNFin1: return (void*)k_ms_finalize<W>;
+    default: return (void*)k_ms_pull<W>;
+  }
+}
+
+template <int W>
+MsParams<W>* ms_node_args(MsArgs<W>& a, int slot) {
+  if (slot == kNRoots || slot == kNList) return &a.base;
+  return slot < kNPush1 ? &a.par[1] : &a.par[0];  // the first half of the body runs odd levels
+}
+
+template <int W>
+cudaKernelNodeParams ms_node_params(MsWorkspace* ws, MsArgs<W>& a, int slot, void** argv) {
+  cudaKernelNodeParams kp = {};
+  kp.func                 = ms_node_fn<W>(slot);
+  argv[0]                 = ms_node_args(a, slot);
+  kp.kernelParams         = argv;
+  kp.blockDim             = dim3(kMsThreads);
+  if (slot == kNRoots) kp.gridDim = dim3(1);
+  else if (slot == kNList) kp.gridDim = dim3(1);
+  else if (slot == kNPush0 || slot == kNPush1) kp.gridDim = dim3(grid_ms(ws, ws->list_cap, kMsWarps));
+  else kp.gridDim = dim3(grid_ms(ws, ws->n_cap, kMsThreads));
+  return kp;
+}
+
+// The pass as a CUDA graph: roots, first frontier list, then
+// WHILE(decide -> SWITCH{push + finalize | pull} for an odd level, the same
+// for the following even level); no host round trip per level.
+template <int W>
+int ms_build_exec(MsWorkspace* ws, MsArgs<W>& a) {
+  MsPassDev*  d = static_cast<MsPassDev*>(ws->pass_dev);
+  cudaGraph_t graph;
+  NWG_CUDA_TRY(cudaGraphCreate(&graph, 0));
+  auto fail = [&](cudaError_t e, const char* what) {
+    cudaGraphDestroy(graph);
+    return cuda_error(e, what);
+  };
+  cudaGraphNode_t* nodes = ws->nodes[W - 1];
+  void*            argv[kNNodes][1];
+  auto add = [&](cudaGraph_t gr, const cudaGraphNode_t* dep, int slot) {
+    cudaKernelNodeParams kp = ms_node_params<W>(ws, a, slot, argv[slot]);
+    return cudaGraphAddKernelNode(&nodes[slot], gr, dep, dep ? 1 : 0, &kp);
+  };
+  cudaError_t e;
+  if ((e = add(graph, nullptr, kNRoots)) != cudaSuccess || (e = add(graph, &nodes[kNRoots], kNList)) != cudaSuccess)
+    return fail(e, "multi-source graph nodes");
+  cudaGraphConditionalHandle h_loop, h_sw[2];
+  if ((e = cudaGraphConditionalHandleCreate(&h_loop, graph, 1, cudaGraphCondAssignDefault)) != cudaSuccess)
+    return fail(e, "loop handle");
+  cudaGraphNodeParams wp = {};
+  wp.type                = cudaGraphNodeTypeConditional;
+  wp.conditional.handle  = h_loop;
+  wp.conditional.type    = cudaGraphCondTypeWhile;
+  wp.conditional.size    = 1;
+  cudaGraphNode_t n_while;
+  if ((e = cudaGraphAddNode(&n_while, graph, &nodes[kNList], 1, &wp)) != cudaSuccess) return fail(e, "while node");
+  cudaGraph_t     body = wp.conditional.phGraph_out[0];
+  cudaGraphNode_t prev = nullptr;
+  int             set_cond = 1;
+  for (int half = 0; half < 2; ++half) {  // half 0: odd level (parity 1), half 1: even level (parity 0)
+    if ((e = cudaGraphConditionalHandleCreate(&h_sw[half], body, 2, cudaGraphCondAssignDefault)) != cudaSuccess)
+      return fail(e, "switch handle");
+    void*                decargs[] = {&d, &h_loop, &h_sw[half], &set_cond};
+    cudaKernelNodeParams dp        = {};
+    dp.func                        = (void*)k_ms_decide;
+    dp.gridDim                     = dim3(1);
+    dp.blockDim                    = dim3(32);
+    dp.kernelParams                = decargs;
+    cudaGraphNode_t n_dec, n_sw;
+    if ((e = cudaGraphAddKernelNode(&n_dec, body, prev ? &prev : nullptr, prev ? 1 : 0, &dp)) != cudaSuccess)
+      return fail(e, "decide node");
+    cudaGraphNodeParams sp = {};
+    sp.type                = cudaGraphNodeTypeConditional;
+    sp.conditional.handle  = h_sw[half];
+    sp.conditional.type    = cudaGraphCondTypeSwitch;
+    sp.conditional.size    = 2;
+    if ((e = cudaGraphAddNode(&n_sw, body, &n_dec, 1, &sp)) != cudaSuccess) return fail(e, "switch node");
+    const int push = half == 0 ? kNPush0 : kNPush1;
+    if ((e = add(sp.conditional.phGraph_out[0], nullptr, push)) != cudaSuccess ||
+        (e = add(sp.conditional.phGraph_out[0], &nodes[push], push + 1)) != cudaSuccess ||
+        (e = add(sp.conditional.phGraph_out[1], nullptr, push + 2)) != cudaSuccess)
+      return fail(e, "level nodes");
+    prev = n_sw;
+  }
+  cudaGraphExec_t exec;
+  if ((e = cudaGraphInstantiate(&exec, graph, 0)) != cudaSuccess) return fail(e, "multi-source graph instantiate");
+  if (ws->tmpl[W - 1]) cudaGraphDestroy(ws->tmpl[W - 1]);
+  ws->tmpl[W - 1] = graph;  // kept: the nodes above belong to it
+  ws->exec[W - 1] = exec;
+  return NWG_OK;
+}
+
+// Points an instantiated pass graph at this pass's graph, depth rows and
+// source masks; rebuilds it if the driver refuses the in-place update.
+template <int W>
+int ms_update_exec(MsWorkspace* ws, MsArgs<W>& a) {
+  if (!ws->exec[W - 1]) return ms_build_exec<W>(ws, a);
+  void* argv[kNNodes][1];
+  for (int slot = 0; slot < kNNodes; ++slot) {
+    cudaKernelNodeParams kp = ms_node_params<W>(ws, a, slot, argv[slot]);
+    if (cudaGraphExecKernelNodeSetParams(ws->exec[W - 1], ws->nodes[W - 1][slot], &kp) != cudaSuccess) {
+      cudaGetLastError();
+      cudaGraphExecDestroy(ws->exec[W - 1]);
+      ws->exec[W - 1] = nullptr;
+      return ms_build_exec<W>(ws, a);
+    }
+  }
+  return NWG_OK;
+}
+
+// Instantiates the pass graph of every word count up front (with arguments
+// of an empty graph; each pass updates them), so no pass pays for it.
+template <int W>
+int ms_prepare(MsWorkspace* ws) {
+  GraphDev  empty;
+  empty.n = 0;
+  empty.m = 0;
+  MsArgs<W> a = ms_args<W>(&empty, ws, nullptr, 0);
+  return ms_build_exec<W>(ws, a);
+}
+
+// The same kernels launched one at a time, the decision read back by the
+// host after each decide (for profilers that cannot see inside conditional
+// graphs).
+template <int W>
+int ms_run_stepped(MsWorkspace* ws, MsArgs<W>& a, cudaStream_t stream) {
+  MsPassDev* d  = static_cast<MsPassDev*>(ws->pass_dev);
+  MsPassDev* hd = static_cast<MsPassDev*>(ws->pass_host);
+  k_ms_roots<W><<<1, kMsThreads, 0, stream>>>(a.base);
+  k_ms_root_list<W><<<1, kMsThreads, 0, stream>>>(a.base);
+  const int g_list = grid_ms(ws, ws->list_cap, kMsWarps);
+  const int g_vert = grid_ms(ws, ws->n_cap, kMsThreads);
+  for (;;) {
+    k_ms_decide<<<1, 32, 0, stream>>>(d, cudaGraphConditionalHandle{}, cudaGraphConditionalHandle{}, 0);
+    NWG_CUDA_TRY(cudaGetLastError());
+    NWG_CUDA_TRY(cudaMemcpyAsync(&hd->level, &d->level, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    NWG_CUDA_TRY(cudaMemcpyAsync(&hd->pull, &d->pull, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    NWG_CUDA_TRY(cudaStreamSynchronize(stream));
+    if (hd->stopped) break;
+    MsParams<W>& q = a.par[hd->level & 1];
+    if (hd->pull) {
+      k_ms_pull<W><<<g_vert, kMsThreads, 0, stream>>>(q);
+    } else {
+      k_ms_push<W><<<g_list, kMsThreads, 0, stream>>>(q);
+      k_ms_finalize<W><<<g_vert, kMsThreads, 0, stream>>>(q);
+    }
+    NWG_CUDA_TRY(cudaGetLastError());
+  }
+  return NWG_OK;
+}
+
+// One pass of up to 64 * W sources: the host writes the pass record (one
+// copy from pinned memory), clears the state, launches the pass graph and
+// reads the record back once at the end.
+template <int W>
+int ms_pass(GraphDev* g, MsWorkspace* ws, const uint32_t* roots_host, uint32_t k, uint8_t* depth_rows, int alpha,
+            cudaStream_t stream, nwg_msbfs_stats* st) {
+  const uint64_t n  = g->n;
+  MsPassDev&     h  = *static_cast<MsPassDev*>(ws->pass_host);
+  MsPassDev*     dd = static_cast<MsPassDev*>(ws->pass_dev);
+  std::memset(&h, 0, sizeof h);
+  h.list_cap  = ws->list_cap;
+  h.k         = k;
+  h.alpha     = alpha;
+  h.unchecked = g->m;
+  std::memcpy(h.roots, roots_host, k * sizeof(uint32_t));
+  // distinct roots form the first frontier; their chunk entries the first list
+  std::vector<uint32_t> uniq(roots_host, roots_host + k);
+  std::sort(uniq.begin(), uniq.end());
+  uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
+  h.nuniq = (uint32_t)uniq.size();
+  std::memcpy(h.uniq, uniq.data(), uniq.size() * sizeof(uint32_t));
+
+  MsArgs<W>    a     = ms_args<W>(g, ws, depth_rows, k);
   const size_t words = (size_t)n * W * sizeof(uint64_t);
   NWG_CUDA_TRY(cudaMemsetAsync(ws->vis, 0, words, stream));
   NWG_CUDA_TRY(cudaMemsetAsync(ws->fr[0], 0, words, stream));
   NWG_CUDA_TRY(cudaMemsetAsync(ws->nx, 0, words, stream));
   NWG_CUDA_TRY(cudaMemsetAsync(depth_rows, 0xFF, (size_t)k * n, stream));
-  k_ms_roots<W><<<(k + 255) / 256, 256, 0, stream>>>(p, roots_dev, k);
-  NWG_CUDA_TRY(cudaGetLastError());
-
-  // distinct roots form the first frontier; their chunk entries the first list
-  std::vector<uint32_t> uniq(roots_host, roots_host + k);
-  std::sort(uniq.begin(), uniq.end());
-  uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
-  NWG_CUDA_TRY(cudaMemcpyAsync(ws->roots_uniq, uniq.data(), uniq.size() * 4, cudaMemcpyHostToDevice, stream));
-  MsCounters& hc = *static_cast<MsCounters*>(ws->cnt_host);
-  NWG_CUDA_TRY(cudaMemsetAsync(ws->cnt, 0, sizeof(MsCounters), stream));
-  p.cnt = static_cast<MsCounters*>(ws->cnt);
-  k_ms_root_list<W><<<1, kMsThreads, 0, stream>>>(p, ws->roots_uniq, (uint32_t)uniq.size());
-  NWG_CUDA_TRY(cudaGetLastError());
-  NWG_CUDA_TRY(cudaMemcpyAsync(&hc, ws->cnt, sizeof(hc), cudaMemcpyDeviceToHost, stream));
+  NWG_CUDA_TRY(cudaMemcpyAsync(dd, &h, sizeof h, cudaMemcpyHostToDevice, stream));
+  if (ws->stepped) {
+    int rc = ms_run_stepped<W>(ws, a, stream);
+    if (rc) return rc;
+  } else {
+    int rc = ms_update_exec<W>(ws, a);
+    if (rc) return rc;
+    NWG_CUDA_TRY(cudaGraphLaunch(ws->exec[W - 1], stream));
+  }
+  NWG_CUDA_TRY(cudaMemcpyAsync(&h, dd, sizeof h, cudaMemcpyDeviceToHost, stream));
   NWG_CUDA_TRY(cudaStreamSynchronize(stream));
-  uint64_t fedges = hc.frontier_edges;
-  std::swap(p.list_cur, p.list_nxt);  // the root list was written as "next"
-  uint64_t nlist     = hc.frontier_count;
-  uint64_t unchecked = g->m;
-  for (uint32_t level = 1;; ++level) {
-    if (level >= 255) return set_error(NWG_EOVERFLOW, "a depth reaches 255: does not fit the uint8 encoding");
-    p.level = level;
-    p.cnt   = static_cast<MsCounters*>(ws->cnt);
-    NWG_CUDA_TRY(cudaMemsetAsync(ws->cnt, 0, sizeof(MsCounters), stream));
-    const bool pull   = fedges > unchecked / (uint64_t)alpha;
-    const bool traced = st->passes == 0 && st->trace_len < NWG_MS_TRACE_CAP;
-    if (traced) NWG_CUDA_TRY(cudaEventRecord(ws->ev_lvl[0], stream));
-    if (pull) {
-      k_ms_pull<W><<<grid_ms(g, 8, n, kMsThreads), kMsThreads, 0, stream>>>(p);
-      st->pull_levels++;
-    } else {
-      unchecked -= std::min(unchecked, fedges);
-      const uint64_t nl = std::min<uint64_t>(nlist, ws->list_cap);
-      k_ms_push<W><<<grid_ms(g, 8, nl, kMsWarps), kMsThreads, 0, stream>>>(p, nl);
-      NWG_CUDA_TRY(cudaGetLastError());
-      k_ms_finalize<W><<<grid_ms(g, 8, n, kMsThreads), kMsThreads, 0, stream>>>(p);
-      st->push_levels++;
+  if (h.status == NWG_EOVERFLOW)
+    return set_error(NWG_EOVERFLOW, "a depth reaches 255: does not fit the uint8 encoding");
+  if (h.status != NWG_OK) return set_error(h.status, "multi-source pass failed");
+  st->levels = std::max(st->levels, h.levels);
+  st->push_levels += h.push_levels;
+  st->pull_levels += h.pull_levels;
+  if (st->passes == 0) {
+    st->trace_len = h.trace_len;
+    for (uint32_t i = 0; i < h.trace_len; ++i) {
+      st->trace_pull[i]           = h.tr_pull[i];
+      st->trace_ms[i]             = (float)((double)(h.tr_t[i + 1] - h.tr_t[i]) * 1e-6);
+      st->trace_frontier_edges[i] = h.tr_fedges[i];
+      st->trace_discovered[i]     = h.tr_disc[i];
     }
-    NWG_CUDA_TRY(cudaGetLastError());
-    if (traced) NWG_CUDA_TRY(cudaEventRecord(ws->ev_lvl[1], stream));
-    NWG_CUDA_TRY(cudaMemcpyAsync(&hc, ws->cnt, sizeof(hc), cudaMemcpyDeviceToHost, stream));
-    NWG_CUDA_TRY(cudaStreamSynchronize(stream));
-    if (traced) {
-      const uint32_t i = st->trace_len++;
-      st->trace_pull[i] = pull ? 1 : 0;
-      cudaEventElapsedTime(&st->trace_ms[i], ws->ev_lvl[0], ws->ev_lvl[1]);
-      st->trace_frontier_edges[i] = fedges;
-      st->trace_discovered[i]     = hc.discovered;
-    }
-    if (hc.discovered == 0) break;
-    st->levels = std::max(st->levels, level + 1);
-    fedges     = hc.frontier_edges;
-    nlist      = hc.frontier_count;
-    std::swap(p.fr_cur, p.fr_nxt);
-    std::swap(p.list_cur, p.list_nxt);
   }
   return NWG_OK;
 }
@@ -441,8 +696,8 @@ int ms_pass(GraphDev* g, MsWorkspace* ws, const uint32_t* roots_dev, const uint3
 uint64_t ms_ws_bytes(uint64_t n_cap, uint64_t m_cap) {
   const uint64_t n = std::max<uint64_t>(n_cap, 1);
   // VIS, FR[2], NX at four words per vertex, two frontier lists (every
-  // frontier vertex has at most deg / kMsChunk + 1 entries), counters, roots
-  return 4 * n * 4 * sizeof(uint64_t) + 2 * (n + m_cap / kMsChunk + 1) * 8 + sizeof(MsCounters) + 2 * 256 * 4;
+  // frontier vertex has at most deg / kMsChunk + 1 entries), the pass record
+  return 4 * n * 4 * sizeof(uint64_t) + 2 * (n + m_cap / kMsChunk + 1) * 8 + sizeof(MsPassDev);
 }
 
 int ms_ws_init_cap(GraphDev* g, uint64_t n_cap, uint64_t m_cap, MsWorkspace* ws) {
@@ -453,20 +708,29 @@ int ms_ws_init_cap(GraphDev* g, uint64_t n_cap, uint64_t m_cap, MsWorkspace* ws)
   ws->n_cap               = n_cap;
   ws->m_cap               = m_cap;
   ws->list_cap            = list_cap;
+  const char* stepped     = std::getenv("NWG_MS_STEPPED");
+  ws->stepped             = stepped && stepped[0] == '1';
+  int dev                 = 0;
+  NWG_CUDA_TRY(cudaGetDevice(&dev));
+  NWG_CUDA_TRY(cudaDeviceGetAttribute(&ws->sm_count, cudaDevAttrMultiProcessorCount, dev));
   if (cudaMalloc(&ws->vis, words) != cudaSuccess || cudaMalloc(&ws->fr[0], words) != cudaSuccess ||
       cudaMalloc(&ws->fr[1], words) != cudaSuccess || cudaMalloc(&ws->nx, words) != cudaSuccess ||
       cudaMalloc(&ws->list[0], list_cap * 8) != cudaSuccess || cudaMalloc(&ws->list[1], list_cap * 8) != cudaSuccess ||
-      cudaMalloc(&ws->cnt, sizeof(MsCounters)) != cudaSuccess || cudaMalloc(&ws->roots, 256 * 4) != cudaSuccess ||
-      cudaMalloc(&ws->roots_uniq, 256 * 4) != cudaSuccess ||
-      cudaMallocHost(&ws->cnt_host, sizeof(MsCounters)) != cudaSuccess) {
+      cudaMalloc(&ws->pass_dev, sizeof(MsPassDev)) != cudaSuccess ||
+      cudaMallocHost(&ws->pass_host, sizeof(MsPassDev)) != cudaSuccess) {
     cudaGetLastError();
     return set_error(NWG_ENOMEM, "multi-source workspace allocation failed");
   }
   NWG_CUDA_TRY(cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking));
   NWG_CUDA_TRY(cudaEventCreate(&ws->ev0));
   NWG_CUDA_TRY(cudaEventCreate(&ws->ev1));
-  NWG_CUDA_TRY(cudaEventCreate(&ws->ev_lvl[0]));
-  NWG_CUDA_TRY(cudaEventCreate(&ws->ev_lvl[1]));
+  if (!ws->stepped) {
+    int rc = ms_prepare<1>(ws);
+    if (!rc) rc = ms_prepare<2>(ws);
+    if (!rc) rc = ms_prepare<3>(ws);
+    if (!rc) rc = ms_prepare<4>(ws);
+    if (rc) return rc;
+  }
   return NWG_OK;
 }
 
@@ -475,20 +739,20 @@ int ms_ws_init(GraphDev* g, MsWorkspace* ws) { return ms_ws_init_cap(g, g->n, g-
 void ms_ws_free(MsWorkspace* ws) {
   if (!ws) return;
   if (ws->stream) cudaStreamSynchronize(ws->stream);
+  for (cudaGraphExec_t e : ws->exec)
+    if (e) cudaGraphExecDestroy(e);
+  for (cudaGraph_t t : ws->tmpl)
+    if (t) cudaGraphDestroy(t);
   cudaFree(ws->vis);
   cudaFree(ws->fr[0]);
   cudaFree(ws->fr[1]);
   cudaFree(ws->nx);
   cudaFree(ws->list[0]);
   cudaFree(ws->list[1]);
-  cudaFree(ws->cnt);
-  cudaFree(ws->roots);
-  cudaFree(ws->roots_uniq);
-  if (ws->cnt_host) cudaFreeHost(ws->cnt_host);
+  cudaFree(ws->pass_dev);
+  if (ws->pass_host) cudaFreeHost(ws->pass_host);
   if (ws->ev0) cudaEventDestroy(ws->ev0);
   if (ws->ev1) cudaEventDestroy(ws->ev1);
-  if (ws->ev_lvl[0]) cudaEventDestroy(ws->ev_lvl[0]);
-  if (ws->ev_lvl[1]) cudaEventDestroy(ws->ev_lvl[1]);
   if (ws->stream) cudaStreamDestroy(ws->stream);
   delete ws;
 }
@@ -505,17 +769,16 @@ int ms_run_on(MsWorkspace* ws, GraphDev* g, const uint32_t* roots_host, uint32_t
   cudaStream_t s = stream ? stream : ws->stream;
   for (uint32_t b = 0; b < k; b += 256) {
     const uint32_t kk = std::min<uint32_t>(256, k - b);
-    NWG_CUDA_TRY(cudaMemcpyAsync(ws->roots, roots_host + b, kk * 4, cudaMemcpyHostToDevice, s));
     uint8_t* rows = depths_dev + (uint64_t)b * g->n;
     int      rc;
     if (kk <= 64) {
-      rc = ms_pass<1>(g, ws, ws->roots, roots_host + b, kk, rows, alpha, s, st);
+      rc = ms_pass<1>(g, ws, roots_host + b, kk, rows, alpha, s, st);
     } else if (kk <= 128) {
-      rc = ms_pass<2>(g, ws, ws->roots, roots_host + b, kk, rows, alpha, s, st);
+      rc = ms_pass<2>(g, ws, roots_host + b, kk, rows, alpha, s, st);
     } else if (kk <= 192) {
-      rc = ms_pass<3>(g, ws, ws->roots, roots_host + b, kk, rows, alpha, s, st);
+      rc = ms_pass<3>(g, ws, roots_host + b, kk, rows, alpha, s, st);
     } else {
-      rc = ms_pass<4>(g, ws, ws->roots, roots_host + b, kk, rows, alpha, s, st);
+      rc = ms_pass<4>(g, ws, roots_host + b, kk, rows, alpha, s, st);
     }
     if (rc) return rc;
     st->passes++;
