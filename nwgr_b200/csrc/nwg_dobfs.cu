@@ -122,73 +122,111 @@ __device__ __forceinline__ void count_entries(const DobfsParams& p, const uint64
 }
 
 // All 32 lanes of the warp must call.  Small entries and the chunk entries
-// of vertices with at most kLaneChunks chunks are written by their own lane;
-// the chunk entries of hubs are written by the whole warp, 32 at a time.
-template <int K>
+// of vertices with at most kLaneChunks chunks are written by their own lane.
+// Hubs (more chunks): with kDefer and hub-record buffers, the warp only
+// records (vertex, first slot, chunk count) -- one atomic per warp -- and the
+// persistent kernel's whole grid writes their entries after the level
+// barrier (expand_hubs); a single SM writing tens of thousands of entries is
+// bound by its outstanding-store limit.  Otherwise the whole warp writes them,
+// 32 at a time.
+template <int K, bool kDefer>
 __device__ __forceinline__ void write_entries(const DobfsParams& p, uint32_t qi, const uint32_t (&v)[K],
-                                              const uint64_t (&d)[K], uint32_t mask, uint64_t spos, uint64_t cpos,
-                                              uint32_t nch) {
+                                              const uint64_t (&d)[K], uint32_t mask, uint64_t spos, uint64_t cpos) {
   CtrlHdr*        c    = &p.ctrl->h;
   const unsigned  lane = threadIdx.x & 31;
   uint32_t* const qs   = p.qs[qi];
   uint64_t* const qc   = p.qc[qi];
+  const uint64_t  scap = p.qs_cap, ccap = p.qc_cap;
   const uint64_t  c0   = cpos;
+  bool            over = false;
   bool            hub  = false;
+  uint32_t        nh   = 0;
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     if (!(mask & (1u << k))) continue;
     if (d[k] < p.th.warp_min) {
-      if (spos < p.qs_cap) {
+      if (spos < scap) {
         qs[spos] = v[k];
       } else {
-        c->status = NWG_EOVERFLOW;
+        over = true;
       }
       ++spos;
     } else {
       const uint64_t nc = chunks_of(d[k], p.th);
       if (nc <= kLaneChunks) {
         for (uint64_t j = 0; j < nc; ++j) {
-          if (cpos + j < p.qc_cap) {
+          if (cpos + j < ccap) {
             qc[cpos + j] = ((uint64_t)v[k] << 32) | j;
           } else {
-            c->status = NWG_EOVERFLOW;
+            over = true;
           }
         }
       } else {
         hub = true;
+        ++nh;
       }
       cpos += nc;
     }
   }
-  unsigned todo = __ballot_sync(kFullMask, hub);
-  while (todo) {
-    const int src = __ffs(todo) - 1;
-    todo &= todo - 1;
-    uint64_t pos = __shfl_sync(kFullMask, c0, src);
+  HubRec* const rec = kDefer ? p.hubrec[qi] : nullptr;
+  if (kDefer && rec != nullptr) {  // uniform: the buffers exist or not
+    uint32_t incl = nh;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t x = __shfl_up_sync(kFullMask, incl, o);
+      if ((int)lane >= o) incl += x;
+    }
+    const uint32_t tot  = __shfl_sync(kFullMask, incl, 31);
+    uint32_t       base = 0;
+    if (tot && lane == 31) base = atomicAdd(&c->nhub[qi], tot);
+    base         = __shfl_sync(kFullMask, base, 31);
+    uint64_t idx = base + incl - nh;
+    uint64_t pos = c0;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      const unsigned valid = __shfl_sync(kFullMask, (mask >> k) & 1u, src);
-      const uint64_t dk    = __shfl_sync(kFullMask, d[k], src);
-      if (valid && dk >= p.th.warp_min) {
-        const uint64_t nc = chunks_of(dk, p.th);
-        if (nc > kLaneChunks) {
-          const uint32_t vk = __shfl_sync(kFullMask, v[k], src);
-          for (uint64_t j = lane; j < nc; j += 32) {
-            if (pos + j < p.qc_cap) {
-              qc[pos + j] = ((uint64_t)vk << 32) | j;
-            } else {
-              c->status = NWG_EOVERFLOW;
+      if (!(mask & (1u << k)) || d[k] < p.th.warp_min) continue;
+      const uint64_t nc = chunks_of(d[k], p.th);
+      if (nc > kLaneChunks) {
+        if (idx < p.hub_cap) {
+          rec[idx] = HubRec{v[k], (uint32_t)nc, pos};
+        } else {
+          over = true;
+        }
+        ++idx;
+      }
+      pos += nc;
+    }
+  } else {
+    unsigned todo = __ballot_sync(kFullMask, hub);
+    while (todo) {
+      const int src = __ffs(todo) - 1;
+      todo &= todo - 1;
+      uint64_t pos = __shfl_sync(kFullMask, c0, src);
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        const unsigned valid = __shfl_sync(kFullMask, (mask >> k) & 1u, src);
+        const uint64_t dk    = __shfl_sync(kFullMask, d[k], src);
+        if (valid && dk >= p.th.warp_min) {
+          const uint64_t nc = chunks_of(dk, p.th);
+          if (nc > kLaneChunks) {
+            const uint32_t vk = __shfl_sync(kFullMask, v[k], src);
+            for (uint64_t j = lane; j < nc; j += 32) {
+              if (pos + j < ccap) {
+                qc[pos + j] = ((uint64_t)vk << 32) | j;
+              } else {
+                over = true;
+              }
             }
           }
+          pos += nc;
         }
-        pos += nc;
       }
     }
   }
-  (void)nch;
+  if (over) c->status = NWG_EOVERFLOW;
 }
 
-template <int K>
+template <int K, bool kDefer>
 __device__ __forceinline__ void append_warp(const DobfsParams& p, uint32_t qi, const uint32_t (&v)[K],
                                             const uint64_t (&d)[K], uint32_t mask, uint32_t& nbig) {
   uint32_t ns, nch, nb;
@@ -202,8 +240,8 @@ __device__ __forceinline__ void append_warp(const DobfsParams& p, uint32_t qi, c
   if ((threadIdx.x & 31) == 31) base = atomicAdd(&p.ctrl->h.qpos[qi], tot);
   base                          = __shfl_sync(kFullMask, base, 31);
   const unsigned long long excl = incl - mine;
-  write_entries<K>(p, qi, v, d, mask, (base & 0xFFFFFFFFull) + (excl & 0xFFFFFFFFull), (base >> 32) + (excl >> 32),
-                   nch);
+  write_entries<K, kDefer>(p, qi, v, d, mask, (base & 0xFFFFFFFFull) + (excl & 0xFFFFFFFFull),
+                           (base >> 32) + (excl >> 32));
 }
 
 // Exclusive block-wide scan of a 64-bit value; all threads call.
@@ -226,7 +264,7 @@ __device__ __forceinline__ unsigned long long block_excl_scan(unsigned long long
   return excl;
 }
 
-template <int K>
+template <int K, bool kDefer>
 __device__ __forceinline__ void append_block(const DobfsParams& p, uint32_t qi, const uint32_t (&v)[K],
                                              const uint64_t (&d)[K], uint32_t mask, uint32_t& nbig) {
   __shared__ unsigned long long s_base;
@@ -240,8 +278,8 @@ __device__ __forceinline__ void append_block(const DobfsParams& p, uint32_t qi, 
   if (threadIdx.x == 0) s_base = atomicAdd(&p.ctrl->h.qpos[qi], tot);
   __syncthreads();
   const unsigned long long base = s_base;
-  write_entries<K>(p, qi, v, d, mask, (base & 0xFFFFFFFFull) + (excl & 0xFFFFFFFFull), (base >> 32) + (excl >> 32),
-                   nch);
+  write_entries<K, kDefer>(p, qi, v, d, mask, (base & 0xFFFFFFFFull) + (excl & 0xFFFFFFFFull),
+                           (base >> 32) + (excl >> 32));
   __syncthreads();
 }
 
@@ -262,6 +300,7 @@ struct TdWarp {
 
 // A warp's winner buffer ran full: degree lookup and append of its entries
 // (all 32 lanes call).
+template <bool kDefer>
 __device__ __forceinline__ void flush_winners(const DobfsParams& p, TdWarp& tw, uint32_t& wcnt, uint32_t nxt,
                                               unsigned long long& scout, uint32_t& nbig) {
   const unsigned lane = threadIdx.x & 31;
@@ -285,7 +324,7 @@ __device__ __forceinline__ void flush_winners(const DobfsParams& p, TdWarp& tw, 
       if (mask & (1u << k)) d[k] = p.off[v[k] + 1] - p.off[v[k]];
 #pragma unroll
     for (int k = 0; k < kVisit; ++k) scout += d[k];
-    append_warp<kVisit>(p, nxt, v, d, mask, nbig);
+    append_warp<kVisit, kDefer>(p, nxt, v, d, mask, nbig);
   }
   wcnt = 0;
   __syncwarp();
@@ -293,6 +332,7 @@ __device__ __forceinline__ void flush_winners(const DobfsParams& p, TdWarp& tw, 
 
 // End of a step: every warp's remaining buffered winners are appended with
 // one reservation for the whole block.  All threads of the block call.
+template <bool kDefer>
 __device__ __forceinline__ void flush_block(const DobfsParams& p, TdWarp* tws, uint32_t wcnt, uint32_t nxt,
                                             unsigned long long& scout, uint32_t& nbig, bool count_scout) {
   __shared__ uint32_t s_cnt[kWarps];
@@ -317,7 +357,7 @@ __device__ __forceinline__ void flush_block(const DobfsParams& p, TdWarp* tws, u
 #pragma unroll
     for (int w = 0; w < kWarps; ++w) scout += d[w];
   }
-  append_block<kWarps>(p, nxt, v, d, mask, nbig);
+  append_block<kWarps, kDefer>(p, nxt, v, d, mask, nbig);
 }
 
 // One batch of top-down edge tests (bfs.hpp:280-289): lane edges u[k] -> v[k]
@@ -327,6 +367,7 @@ __device__ __forceinline__ void flush_block(const DobfsParams& p, TdWarp* tws, u
 // atomicOr (all issued before any result is used).  A claim's winner writes parents[v] = u (the reference's CAS
 // winner) and is buffered; scout and the next queue are updated when the
 // buffer is flushed.  All 32 lanes must call.
+template <bool kDefer>
 __device__ __forceinline__ void visit_batch(const DobfsParams& p, uint32_t* __restrict__ parents, uint32_t nxt,
                                             const uint32_t (&u)[kVisit], const uint32_t (&v)[kVisit], uint32_t valid,
                                             TdWarp& tw, uint32_t& wcnt, unsigned long long& scout, uint32_t& nbig) {
@@ -361,7 +402,7 @@ __device__ __forceinline__ void visit_batch(const DobfsParams& p, uint32_t* __re
     }
   }
   wcnt += tot;
-  if (wcnt > kWinBuf - 32 * kVisit) flush_winners(p, tw, wcnt, nxt, scout, nbig);
+  if (wcnt > kWinBuf - 32 * kVisit) flush_winners<kDefer>(p, tw, wcnt, nxt, scout, nbig);
 }
 
 // Largest range index whose exclusive prefix (in `excl`) is <= e.
@@ -380,6 +421,7 @@ __device__ __forceinline__ int owner_of(const uint32_t* excl, uint32_t e) {
 // range) per lane per batch; the heads and tails (< 4 edges each) are dealt
 // out as scalar edges, kVisit per lane per batch.  A unit's range is found by
 // binary search over the prefix in shared memory.  All 32 lanes must call.
+template <bool kDefer>
 __device__ __forceinline__ void gather_ranges(const DobfsParams& p, uint32_t* __restrict__ parents, uint32_t nxt,
                                               uint32_t u, uint64_t lo, uint64_t hi, TdWarp& tw, uint32_t& wcnt,
                                               unsigned long long& scout, uint32_t& nbig) {
@@ -419,7 +461,7 @@ __device__ __forceinline__ void gather_ranges(const DobfsParams& p, uint32_t* __
       vv[3] = x.w;
       valid = 0xFu;
     }
-    visit_batch(p, parents, nxt, uu, vv, valid, tw, wcnt, scout, nbig);
+    visit_batch<kDefer>(p, parents, nxt, uu, vv, valid, tw, wcnt, scout, nbig);
   }
   for (uint32_t j = 0; j < stot; j += 32 * kVisit) {
     uint32_t uu[kVisit], vv[kVisit], valid = 0;
@@ -437,7 +479,7 @@ __device__ __forceinline__ void gather_ranges(const DobfsParams& p, uint32_t* __
         valid |= 1u << k;
       }
     }
-    visit_batch(p, parents, nxt, uu, vv, valid, tw, wcnt, scout, nbig);
+    visit_batch<kDefer>(p, parents, nxt, uu, vv, valid, tw, wcnt, scout, nbig);
   }
   __syncwarp();
 }
@@ -472,6 +514,13 @@ __device__ __forceinline__ void init_step(const DobfsParams& p, uint32_t root, u
   }
   const uint32_t rw = root >> 5;
   for (uint64_t w = tid; w < p.nwords; w += stride) p.V[w] = (w == rw) ? (1u << (root & 31)) : 0u;
+  {  // a hub root's chunk entries, written by the whole grid
+    const uint64_t rdeg = p.off[root + 1] - p.off[root];
+    if (rdeg >= p.th.warp_min) {
+      const uint64_t nc = chunks_of(rdeg, p.th);
+      for (uint64_t j = tid; j < nc && j < p.qc_cap; j += stride) p.qc[0][j] = ((uint64_t)root << 32) | j;
+    }
+  }
 
   if (tid == 0) {
     CtrlHdr&       c   = p.ctrl->h;
@@ -493,11 +542,10 @@ __device__ __forceinline__ void init_step(const DobfsParams& p, uint32_t root, u
       p.qs[0][0] = root;
       c.qpos[0]  = 1;
     } else {
-      const uint64_t nc = chunks_of(deg, p.th);
-      for (uint64_t j = 0; j < nc && j < p.qc_cap; ++j) p.qc[0][j] = ((uint64_t)root << 32) | j;
-      c.qpos[0] = nc << 32;
+      c.qpos[0] = chunks_of(deg, p.th) << 32;  // entries written above
       c.qbig[0] = 1;
     }
+    c.nhub[0] = c.nhub[1] = 0;
     c.cur       = 0;
     c.bm        = 1;
     c.bu_mode   = 0;
@@ -629,6 +677,7 @@ __device__ uint32_t decide_core(const DobfsParams& p) {
       const uint32_t nxt = c.cur ^ 1u;
       c.qpos[nxt] = 0;
       c.qbig[nxt] = 0;
+      c.nhub[nxt] = 0;
       c.acc_scout = 0;
       // warp work units of the step: chunk entries + groups of 32 small vertices
       const uint64_t units = (c.qpos[c.cur] >> 32) + ((c.qpos[c.cur] & 0xFFFFFFFFull) + 31) / 32;
@@ -675,7 +724,10 @@ __global__ void k_decide(DobfsParams p) {
 // hubs spread over the grid), then the small-degree queue; both go through
 // gather_ranges, a group of entries per warp.  The group size of chunk
 // entries shrinks when there are few so every warp gets work.
-__device__ __forceinline__ void td_step(const DobfsParams& p, TdWarp* tws, uint32_t block, uint32_t nblocks) {
+// Returns the queue buffer the step wrote (read before any barrier that lets
+// the decide kernel swap the buffers).
+template <bool kDefer>
+__device__ __forceinline__ uint32_t td_step(const DobfsParams& p, TdWarp* tws, uint32_t block, uint32_t nblocks) {
   CtrlHdr*           c       = &p.ctrl->h;
   const uint32_t     cur     = __ldcg(&c->cur);
   const uint32_t     nxt     = cur ^ 1u;
@@ -705,7 +757,7 @@ __device__ __forceinline__ void td_step(const DobfsParams& p, TdWarp* tws, uint3
       lo = ob + (ent & 0xFFFFFFFFull) * p.th.chunk;
       hi = min(oe, lo + p.th.chunk);
     }
-    gather_ranges(p, parents, nxt, u, lo, hi, tw, wcnt, scout, nbig);
+    gather_ranges<kDefer>(p, parents, nxt, u, lo, hi, tw, wcnt, scout, nbig);
   }
 
   const uint32_t* qs = p.qs[cur];
@@ -718,9 +770,9 @@ __device__ __forceinline__ void td_step(const DobfsParams& p, TdWarp* tws, uint3
       lo = p.off[u];
       hi = p.off[u + 1];
     }
-    gather_ranges(p, parents, nxt, u, lo, hi, tw, wcnt, scout, nbig);
+    gather_ranges<kDefer>(p, parents, nxt, u, lo, hi, tw, wcnt, scout, nbig);
   }
-  flush_block(p, tws, wcnt, nxt, scout, nbig, true);
+  flush_block<kDefer>(p, tws, wcnt, nxt, scout, nbig, true);
 
   const unsigned long long tot = block_sum(scout);
   __syncthreads();
@@ -729,12 +781,13 @@ __device__ __forceinline__ void td_step(const DobfsParams& p, TdWarp* tws, uint3
     if (tot) atomicAdd(&c->acc_scout, tot);
     if (nb) atomicAdd(&c->qbig[nxt], nb);
   }
+  return nxt;
 }
 
 // k_td: one top-down step over the whole grid.
 __global__ void __launch_bounds__(kThreads, 3) k_td(DobfsParams p) {
   __shared__ TdWarp s_tw[kWarps];
-  td_step(p, s_tw, blockIdx.x, gridDim.x);
+  td_step<false>(p, s_tw, blockIdx.x, gridDim.x);
 }
 
 // Grid-wide barrier of a cooperative launch.  The wait is bounded: after
@@ -787,12 +840,35 @@ __device__ __forceinline__ bool grid_barrier(const DobfsParams& p, unsigned nblo
 // and the direction stays top-down; it then leaves the next decision for
 // the graph's decide node (pre_decided).  Long, thin traversals (grids,
 // roads) thus pay a barrier per level instead of two kernel launches.
+// Writes the chunk entries of the hub records the level deferred (queue
+// buffer qi): a warp per record, grid-strided, so the writes come from every
+// SM.  Runs after the level's barrier, beside the decision; the next barrier
+// (or the kernel's end) orders them before the next level reads the queue.
+__device__ __forceinline__ void expand_hubs(const DobfsParams& p, uint32_t qi, uint32_t block, uint32_t nblocks) {
+  const HubRec* rec = p.hubrec[qi];
+  if (rec == nullptr) return;
+  const uint64_t  nrec   = min((uint64_t)__ldcg(&p.ctrl->h.nhub[qi]), p.hub_cap);
+  const unsigned  lane   = threadIdx.x & 31;
+  const uint64_t  gwarp  = (uint64_t)block * kWarps + (threadIdx.x >> 5);
+  const uint64_t  nwarps = (uint64_t)nblocks * kWarps;
+  uint64_t* const qc     = p.qc[qi];
+  static_assert(sizeof(HubRec) == 16, "one 16-byte load per record");
+  for (uint64_t r = gwarp; r < nrec; r += nwarps) {
+    // L2 loads: the records were written by other SMs during this launch
+    const uint4    raw = __ldcg(reinterpret_cast<const uint4*>(rec) + r);
+    const uint64_t pos = (uint64_t)raw.z | ((uint64_t)raw.w << 32);
+    for (uint64_t j = lane; j < raw.y; j += 32)
+      if (pos + j < p.qc_cap) qc[pos + j] = ((uint64_t)raw.x << 32) | j;
+  }
+}
+
 __global__ void __launch_bounds__(kThreads) k_td_loop(DobfsParams p) {
   __shared__ TdWarp   s_tw[kWarps];
   __shared__ uint32_t s_next;
   for (;;) {
-    td_step(p, s_tw, blockIdx.x, gridDim.x);
+    const uint32_t wrote = td_step<true>(p, s_tw, blockIdx.x, gridDim.x);
     if (!grid_barrier(p, gridDim.x)) break;
+    expand_hubs(p, wrote, blockIdx.x, gridDim.x);
     if (blockIdx.x == 0 && threadIdx.x == 0) s_next = decide_core(p);
     if (!grid_barrier(p, gridDim.x)) break;
     if (threadIdx.x == 0) s_next = __ldcg(&p.ctrl->h.action);
@@ -982,13 +1058,13 @@ __device__ __forceinline__ void b2q_step(const DobfsParams& p, TdWarp* s_tw, uin
     const uint64_t vbase = t * kTileWords * 32;
     for (uint32_t j = 0; j < total; j += 32) {
       const uint32_t k = min(32u, total - j);  // warp-uniform
-      if (wcnt + k > kWinBuf) flush_winners(p, tw, wcnt, qi, scout, nbig);
+      if (wcnt + k > kWinBuf) flush_winners<false>(p, tw, wcnt, qi, scout, nbig);
       if (lane < k) tw.win[wcnt + lane] = (uint32_t)(vbase + list[j + lane]);
       wcnt += k;
     }
     __syncwarp();
   }
-  flush_block(p, s_tw, wcnt, qi, scout, nbig, false);
+  flush_block<false>(p, s_tw, wcnt, qi, scout, nbig, false);
   const uint32_t nb = block_sum(nbig);
   if (threadIdx.x == 0 && nb) atomicAdd(&c->qbig[qi], nb);
 }
@@ -1114,7 +1190,7 @@ __global__ void __launch_bounds__(kThreads) k_ragged(RaggedParams rp) {
       } else if (next == kActB2Q) {
         b2q_step(p, s_tw, 0, 1);
       } else {
-        td_step(p, s_tw, 0, 1);
+        td_step<false>(p, s_tw, 0, 1);
       }
       __syncthreads();
     }
@@ -1244,6 +1320,8 @@ int ws_init(GraphDev* g, Workspace* ws) {
   const uint64_t qs_cap = std::max<uint64_t>(n, 1);
   const uint64_t big    = std::min<uint64_t>(n, m / g->th.warp_min);
   const uint64_t qc_cap = std::max<uint64_t>(1, m / g->th.chunk + big + 1);
+  // deferred hubs have more than kLaneChunks chunks: out-degree > chunk * kLaneChunks
+  const uint64_t hub_cap = m / ((uint64_t)g->th.chunk * kLaneChunks) + 1;
 
   NWG_CUDA_TRY(cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking));
   NWG_CUDA_TRY(cudaEventCreate(&ws->ev0));
@@ -1252,6 +1330,7 @@ int ws_init(GraphDev* g, Workspace* ws) {
       cudaMalloc(&ws->V, 3ull * std::max<uint32_t>(nwords, 1) * sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(&ws->qbuf, 2ull * qs_cap * sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(&ws->cbuf, 2ull * qc_cap * sizeof(uint64_t)) != cudaSuccess ||
+      cudaMalloc(&ws->hubbuf, 2ull * hub_cap * sizeof(HubRec)) != cudaSuccess ||
       cudaMalloc(&ws->ctrl, sizeof(Ctrl)) != cudaSuccess) {
     cudaGetLastError();
     return set_error(NWG_ENOMEM, "workspace allocation failed (n=" + std::to_string(n) + ")");
@@ -1277,6 +1356,9 @@ int ws_init(GraphDev* g, Workspace* ws) {
   P.qc[1]        = ws->cbuf + qc_cap;
   P.qs_cap       = qs_cap;
   P.qc_cap       = qc_cap;
+  P.hubrec[0]    = ws->hubbuf;
+  P.hubrec[1]    = ws->hubbuf + hub_cap;
+  P.hub_cap      = hub_cap;
   P.th           = g->th;
   P.ctrl         = ws->ctrl;
   return build_exec(ws);
@@ -1297,6 +1379,7 @@ void ws_free(Workspace* ws) {
   cudaFree(ws->V);
   cudaFree(ws->qbuf);
   cudaFree(ws->cbuf);
+  cudaFree(ws->hubbuf);
   cudaFree(ws->ctrl);
   if (ws->ctrl_host) cudaFreeHost(ws->ctrl_host);
   cudaSetDevice(prev);

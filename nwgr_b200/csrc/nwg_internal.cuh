@@ -63,6 +63,7 @@ struct alignas(16) CtrlHdr {
 
   unsigned long long qpos[2];    // [buffer] small entries | chunk entries << 32
   uint32_t           qbig[2];    // [buffer] vertices in the chunk queue
+  uint32_t           nhub[2];    // [buffer] hub records whose chunk entries are still to be written
   uint32_t cur;                  // queue buffer holding the frontier
   uint32_t bm;                   // bottom-up: index of the bitmap holding the latest pull's discoveries
   uint32_t bu_mode;              // 0: first pull of a phase (front = visited), 1: later pull (front = C[bm])
@@ -94,6 +95,15 @@ struct Ctrl {
   unsigned long long t_first_decide;
 };
 
+// A vertex with many chunk entries discovered by the persistent small-level
+// kernel: its entries qc[pos .. pos + nc) are written by the whole grid after
+// the level's barrier instead of by the one warp that claimed it.
+struct HubRec {
+  uint32_t v;
+  uint32_t nc;
+  uint64_t pos;
+};
+
 // Static parameters of the level-loop kernels (baked into the CUDA graph).
 struct DobfsParams {
   const uint64_t* off;     // out-CSR offsets [n+1]
@@ -111,6 +121,8 @@ struct DobfsParams {
   uint64_t*       qc[2];  // chunk queues
   uint64_t        qs_cap;
   uint64_t        qc_cap;
+  HubRec*         hubrec[2];  // [buffer] deferred hub records (null: hubs are written by their warp)
+  uint64_t        hub_cap;
   Thresholds      th;
   Ctrl*           ctrl;
   cudaGraphConditionalHandle h_loop;
@@ -128,6 +140,7 @@ struct Workspace {
   uint32_t*       V = nullptr;        // V, C0, C1 in one allocation
   uint32_t*       qbuf = nullptr;     // both small queues
   uint64_t*       cbuf = nullptr;     // both chunk queues
+  HubRec*         hubbuf = nullptr;   // both deferred-hub record lists
   Ctrl*           ctrl = nullptr;     // device
   Ctrl*           ctrl_host = nullptr;  // pinned mirror for stats
   cudaStream_t    stream = nullptr;   // owned stream for the synchronous API
