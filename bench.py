@@ -73,6 +73,7 @@ def parse():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-ragged", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-verify", action="store_true")
     ap.add_argument("--serve-slots", type=int, default=16)
     ap.add_argument("--profile-one", action="store_true",
                     help="after warm-up, run one traversal inside an NVTX range 'nwg_profile' and exit (for ncu)")
@@ -339,6 +340,35 @@ def bench_ragged(nwg, torch, num_graphs=1000, reps=3):
             "classes": {k: v.__dict__ for k, v in params.items()}, "generate_s": gen_s, "autotune_s": tune_s}
 
 
+def bench_verifier(nwg, torch, g, roots, with_cpu):
+    """Device BFSVerifier (nwg_verify) on the bench graph: device time of the
+    check (its own top-down BFS plus the per-vertex parent checks) for the
+    first roots' device parents, beside the reference's BFSVerifier
+    (bfs.hpp:44-98, oracle/_ref) on the host for the first root."""
+    par = torch.empty(g.n, dtype=torch.int32, device="cuda")
+    out = {"roots": [], "device_ms": [], "valid": []}
+    for r in roots[:4]:
+        nwg.bfs_device(g, int(r), par)
+        res = nwg.verify(g, int(r), par)
+        out["roots"].append(int(r))
+        out["device_ms"].append(float(res.device_ms))
+        out["valid"].append(bool(res.valid))
+    if with_cpu:
+        from oracle.oracle import Reference
+
+        off, cols = g.csr()
+        nwg.bfs_device(g, int(roots[0]), par)
+        host = par.cpu().numpy().view(np.uint32)
+        ref = Reference()
+        rg = ref.graph(off, cols)
+        t0 = time.perf_counter()
+        ok = rg.verify(int(roots[0]), host)
+        out["reference_cpu_ms"] = 1e3 * (time.perf_counter() - t0)
+        out["reference_valid"] = bool(ok)
+        rg.close()
+    return out
+
+
 SERVE_RATES = (1000, 10000, 50000, 100000, 200000)
 
 
@@ -521,6 +551,9 @@ def main():
                "d2h_bytes_per_step": int(4 * n * len(roots)),
                "note": "per step: upload CSR from pinned host memory, 64 nwg_bfs calls each returning parents "
                        "to pinned host memory, release"}
+    verifier = None
+    if not args.no_verify:
+        verifier = bench_verifier(nwg, torch, g, roots, rank == 0 and not args.no_cpu)
     batched = None
     if not args.no_batched:
         ws.close()
@@ -568,7 +601,7 @@ def main():
                                          "scaled by directed entries" if traffic else None},
             "gpu_launches": int(np.sum(launches)) * args.steps,
             "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, "batched": batched, "ragged": ragged,
-            "serving": serving,
+            "serving": serving, "verifier": verifier,
         }
         print(json.dumps(line), flush=True)
     if ws is not None:

@@ -274,6 +274,25 @@ int nwg_server_run_trace(nwg_server s, uint32_t count, const uint32_t* graph, co
 int nwg_bfs_noalloc(const uint64_t* out_off, const uint32_t* out_col, const uint64_t* in_off, const uint32_t* in_col,
                     uint64_t n, uint32_t root, int alpha, int beta, uint32_t* parents_dev, void* stream);
 
+/* Device BFSVerifier: the checks of nw::graph::BFSVerifier(g, g_t, source,
+ * parent) (reference: include/nwgraph/algorithms/bfs.hpp:44-98) on the GPU,
+ * for a parent array in host OR device memory (exactly one non-NULL).  Depths
+ * come from a plain top-down BFS written only for this check.  valid = 1 when
+ * the reference verifier would return true; otherwise first_bad is the
+ * lowest failing vertex (the one the reference stops at) and reason the
+ * reference's failure: 1 source wrong, 2 wrong depths, 3 no edge from the
+ * parent, 4 reachability mismatch.  Synchronous. */
+typedef struct {
+  int32_t valid;
+  uint32_t reason;
+  uint64_t first_bad;
+  uint64_t reached; /* vertices reachable from the source */
+  uint32_t levels;  /* BFS levels of the check's own traversal */
+  float device_ms;
+} nwg_verify_result;
+int nwg_verify(nwg_graph g, uint32_t source, const uint32_t* parents_host, const uint32_t* parents_dev,
+               nwg_verify_result* result);
+
 /* Seeded synthetic graph generators on the device (no reference
  * counterpart: NWGraph ships no RMAT/uniform/grid generator).  Each builds a
  * symmetrized, self-loop-free, deduplicated CSR with sorted rows directly in

@@ -41,6 +41,7 @@ EXPORTED = (
     "nwg_gen_grid", "nwg_pick_roots", "nwg_bfs_noalloc", "nwg_msbfs_ws_create", "nwg_msbfs_ws_destroy",
     "nwg_msbfs", "nwg_ragged_register", "nwg_ragged_release", "nwg_ragged_info", "nwg_ragged_bfs",
     "nwg_server_create", "nwg_server_destroy", "nwg_server_submit", "nwg_server_wait", "nwg_server_run_trace",
+    "nwg_verify",
 )
 
 
@@ -121,6 +122,14 @@ class ServerStats(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class VerifyResult(C.Structure):
+    _fields_ = [("valid", C.c_int32), ("reason", C.c_uint32), ("first_bad", C.c_uint64), ("reached", C.c_uint64),
+                ("levels", C.c_uint32), ("device_ms", C.c_float)]
+
+    REASONS = {0: "ok", 1: "source wrong", 2: "wrong depths", 3: "no edge from the parent",
+               4: "reachability mismatch"}
+
+
 _vp = C.c_void_p
 _u32, _u64, _int = C.c_uint32, C.c_uint64, C.c_int
 
@@ -162,6 +171,7 @@ def _load():
         "nwg_server_submit": (_int, [_vp, _u32, _u32, _vp, C.POINTER(_u64)]),
         "nwg_server_wait": (_int, [_vp, _u64, C.POINTER(C.c_double)]),
         "nwg_server_run_trace": (_int, [_vp, _u32, _vp, _vp, _vp, _vp, _vp, _vp, C.POINTER(ServerStats)]),
+        "nwg_verify": (_int, [_vp, _u32, _vp, _vp, C.POINTER(VerifyResult)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -544,6 +554,20 @@ def depths_from_parents(parents: np.ndarray, root: int) -> np.ndarray:
         pending = pending[~ready]
         d += 1
     return depth
+
+
+def verify(g: Graph, root: int, parents) -> VerifyResult:
+    """nw::graph::BFSVerifier on the GPU (bfs.hpp:44-98): parents is a host
+    uint32 array or a device tensor.  Returns the VerifyResult (valid, and
+    for an invalid array the lowest failing vertex and the reason)."""
+    r = VerifyResult()
+    if isinstance(parents, np.ndarray):
+        p = np.ascontiguousarray(parents, dtype=np.uint32)
+        assert p.size >= g.n
+        check(lib.nwg_verify(g.h, int(root), p.ctypes.data, None, C.byref(r)))
+    else:
+        check(lib.nwg_verify(g.h, int(root), None, _ptr(parents), C.byref(r)))
+    return r
 
 
 def bfs_verifier(off, cols, root, parents, in_off=None, in_cols=None) -> bool:
