@@ -274,6 +274,25 @@ int nwg_server_run_trace(nwg_server s, uint32_t count, const uint32_t* graph, co
 int nwg_bfs_noalloc(const uint64_t* out_off, const uint32_t* out_col, const uint64_t* in_off, const uint32_t* in_col,
                     uint64_t n, uint32_t root, int alpha, int beta, uint32_t* parents_dev, void* stream);
 
+/* Graph files into the registry (read on the host, uploaded once like
+ * nwg_graph_register).  The format is recognised from the content:
+ *  - MatrixMarket, as NWGraph's read_mm reads it (io/mmio.hpp:60-103,
+ *    172-208): coordinate general|symmetric, 1-based ids, a symmetric file
+ *    contributes both directions of each off-diagonal entry, self-loops and
+ *    duplicates kept, values ignored, n = max(rows, cols, largest id);
+ *  - NWGraph's binary adjacency, as index_adjacency::serialize writes it
+ *    (adjacency.hpp:158-162, containers/compressed.hpp:303-312; 4- or
+ *    8-byte offsets, the first array = 4-byte target ids); n is taken from
+ *    the offsets count (the 8-byte N_ field is not the vertex count and,
+ *    with 4-byte offsets, half of it is not written from N_ at all).
+ * Rows are sorted by target.  The in-CSR is the transpose, or the out-CSR
+ * itself for a symmetric MatrixMarket file or with NWG_READ_SYMMETRIC. */
+#define NWG_READ_SYMMETRIC 0x1u
+int nwg_graph_read(const char* path, uint32_t flags, nwg_graph* out);
+/* Writes a registered graph's out-CSR in NWGraph's binary adjacency format
+ * (8-byte offsets), readable by index_adjacency::deserialize. */
+int nwg_graph_write_nwbin(nwg_graph g, const char* path);
+
 /* Device BFSVerifier: the checks of nw::graph::BFSVerifier(g, g_t, source,
  * parent) (reference: include/nwgraph/algorithms/bfs.hpp:44-98) on the GPU,
  * for a parent array in host OR device memory (exactly one non-NULL).  Depths

@@ -41,7 +41,7 @@ EXPORTED = (
     "nwg_gen_grid", "nwg_pick_roots", "nwg_bfs_noalloc", "nwg_msbfs_ws_create", "nwg_msbfs_ws_destroy",
     "nwg_msbfs", "nwg_ragged_register", "nwg_ragged_release", "nwg_ragged_info", "nwg_ragged_bfs",
     "nwg_server_create", "nwg_server_destroy", "nwg_server_submit", "nwg_server_wait", "nwg_server_run_trace",
-    "nwg_verify",
+    "nwg_verify", "nwg_graph_read", "nwg_graph_write_nwbin",
 )
 
 
@@ -172,6 +172,8 @@ def _load():
         "nwg_server_wait": (_int, [_vp, _u64, C.POINTER(C.c_double)]),
         "nwg_server_run_trace": (_int, [_vp, _u32, _vp, _vp, _vp, _vp, _vp, _vp, C.POINTER(ServerStats)]),
         "nwg_verify": (_int, [_vp, _u32, _vp, _vp, C.POINTER(VerifyResult)]),
+        "nwg_graph_read": (_int, [C.c_char_p, _u32, C.POINTER(_vp)]),
+        "nwg_graph_write_nwbin": (_int, [_vp, C.c_char_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -252,6 +254,17 @@ class Graph:
             in_cols = np.ascontiguousarray(in_cols, dtype=np.uint32)
         check(fn(_ptr(off), _ptr(cols), off.size - 1, _ptr(in_off), _ptr(in_cols), flags, C.byref(h)))
         return cls(h.value)
+
+    @classmethod
+    def read(cls, path: str, symmetric: bool = False) -> "Graph":
+        """MatrixMarket or NWGraph binary adjacency file (nwg_graph_read)."""
+        h = _vp()
+        check(lib.nwg_graph_read(os.fsencode(path), 1 if symmetric else 0, C.byref(h)))
+        return cls(h.value)
+
+    def write_nwbin(self, path: str) -> None:
+        """The out-CSR in NWGraph's binary adjacency format."""
+        check(lib.nwg_graph_write_nwbin(self.h, os.fsencode(path)))
 
     @classmethod
     def rmat(cls, scale: int, edge_factor: int = 16, seed: int = 1, a=0.57, b=0.19, c=0.19):

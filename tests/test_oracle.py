@@ -201,3 +201,31 @@ def test_mtx_reader_follows_read_mm():
     for name, (n, m) in want.items():
         nn, u, v = O.read_mtx(os.path.join(base, name + ".mtx"))
         assert (nn, u.size) == (n, m)
+
+
+def test_nwbin_fixtures_follow_the_reference_layout(golden):
+    """tests/golden/*.nwbin were written by NWGraph's serializers: vertex
+    count, is_open, magic, the 8-byte N_ field (N + 1 after fill; with 4-byte
+    offsets only its low half comes from N_), offsets, then the target ids."""
+    import struct
+
+    by = {G.name: G for G in golden}
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    for name in ("karate", "bktest2", "sherman4"):
+        for kind, osz in (("a0", 4), ("u64", 8)):
+            d = open(os.path.join(here, f"{name}.{kind}.nwbin"), "rb").read()
+            vcount, = struct.unpack_from("<Q", d, 0)
+            assert d[9:43] == b"NW GRAPH indexed_struct_of_arrays\x00"
+            nfield, noff, offsz = struct.unpack_from("<QQQ", d, 43)
+            assert offsz == osz and noff == vcount + 1
+            assert (nfield & ((1 << (8 * osz)) - 1)) == noff
+            at = 67
+            off = np.frombuffer(d, np.uint32 if osz == 4 else np.uint64, noff, at).astype(np.uint64)
+            at += noff * osz
+            m, narrays, cnt, elsz = struct.unpack_from("<QQQQ", d, at)
+            assert narrays == 1 and cnt == m and elsz == 4
+            cols = np.frombuffer(d, np.uint32, m, at + 32)
+            G = by[name]
+            assert np.array_equal(off, G.off)
+            rows = [np.sort(cols[off[u]:off[u + 1]]) for u in range(vcount)]
+            assert np.array_equal(np.concatenate(rows), G.cols)
