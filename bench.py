@@ -74,6 +74,7 @@ def parse():
     ap.add_argument("--no-ragged", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-verify", action="store_true")
+    ap.add_argument("--no-bc", action="store_true")
     ap.add_argument("--serve-slots", type=int, default=16)
     ap.add_argument("--profile-one", action="store_true",
                     help="after warm-up, run one traversal inside an NVTX range 'nwg_profile' and exit (for ncu)")
@@ -369,6 +370,35 @@ def bench_verifier(nwg, torch, g, roots, with_cpu):
     return out
 
 
+def bench_bc(nwg, scale=22, k=64, cpu_sample=4, with_cpu=True):
+    """Approximate betweenness centrality (brandes_bc<float, double>) on
+    RMAT-`scale` from k seeded sources: device time of nwg_bc, beside the
+    reference's parallel brandes_bc on this host for the first cpu_sample
+    sources (oracle/_ref, all host threads)."""
+    g = nwg.Graph.rmat(scale, 16, seed=GRAPH_SEED)
+    src = g.roots(k, seed=ROOT_SEED)
+    nwg.betweenness(g, src[:4])  # warm-up
+    times = []
+    for _ in range(3):
+        _, st = nwg.betweenness(g, src)
+        times.append(st.device_ms)
+    out = {"graph": f"RMAT-{scale} ef16", "sources": int(k), "device_ms": float(np.median(times)),
+           "ms_per_source": float(np.median(times)) / k, "levels": int(st.max_levels), "lanes": int(st.lanes)}
+    if with_cpu:
+        from oracle.oracle import Reference
+
+        off, cols = g.csr()
+        ref = Reference()
+        rg = ref.graph(off, cols)
+        _, secs = rg.bc(src[:cpu_sample])
+        rg.close()
+        out["reference_cpu_ms_per_source"] = 1e3 * secs / cpu_sample
+        out["reference_threads"] = ref.threads()
+        out["speedup_per_source"] = out["reference_cpu_ms_per_source"] / out["ms_per_source"]
+    g.release()
+    return out
+
+
 SERVE_RATES = (1000, 10000, 50000, 100000, 200000)
 
 
@@ -574,6 +604,13 @@ def main():
             g.release()
             ws, g = None, None
         serving = bench_serving(nwg, slots=args.serve_slots)
+    bc = None
+    if not args.no_bc:
+        if ws is not None:
+            ws.close()
+            g.release()
+            ws, g = None, None
+        bc = bench_bc(nwg, with_cpu=rank == 0 and not args.no_cpu)
     cpu = None
     if rank == 0 and not args.no_cpu:
         if g is None:
@@ -601,7 +638,7 @@ def main():
                                          "scaled by directed entries" if traffic else None},
             "gpu_launches": int(np.sum(launches)) * args.steps,
             "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, "batched": batched, "ragged": ragged,
-            "serving": serving, "verifier": verifier,
+            "serving": serving, "verifier": verifier, "betweenness": bc,
         }
         print(json.dumps(line), flush=True)
     if ws is not None:

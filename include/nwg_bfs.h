@@ -274,6 +274,26 @@ int nwg_server_run_trace(nwg_server s, uint32_t count, const uint32_t* graph, co
 int nwg_bfs_noalloc(const uint64_t* out_off, const uint32_t* out_col, const uint64_t* in_off, const uint32_t* in_col,
                     uint64_t n, uint32_t root, int alpha, int beta, uint32_t* parents_dev, void* stream);
 
+/* Approximate betweenness centrality over `k` sources (Brandes): the
+ * computation of nw::graph::brandes_bc<float, double>(graph, sources,
+ * threads, ..., normalize) (reference: include/nwgraph/algorithms/
+ * betweenness_centrality.hpp:218-324) on the out-graph: per source a BFS
+ * with double path counts, then float dependencies accumulated deepest
+ * level first, every reached vertex (the source included) adding its own;
+ * scores divided by the largest when normalize != 0.  `lanes` sources run
+ * at once (0 = 4, at most 16), one stream each.  Scores (n floats) go to
+ * scores_host and/or scores_dev; float sums across sources, as in the
+ * reference, so results agree with it within the reference verifier's
+ * tolerance (1e-6 on normalized scores), not bit for bit. */
+typedef struct {
+  uint32_t sources;
+  uint32_t lanes;
+  uint32_t max_levels;
+  float device_ms;
+} nwg_bc_stats;
+int nwg_bc(nwg_graph g, const uint32_t* sources, uint32_t k, int normalize, uint32_t lanes, float* scores_host,
+           float* scores_dev, nwg_bc_stats* stats);
+
 /* Graph files into the registry (read on the host, uploaded once like
  * nwg_graph_register).  The format is recognised from the content:
  *  - MatrixMarket, as NWGraph's read_mm reads it (io/mmio.hpp:60-103,

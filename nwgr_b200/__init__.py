@@ -41,7 +41,7 @@ EXPORTED = (
     "nwg_gen_grid", "nwg_pick_roots", "nwg_bfs_noalloc", "nwg_msbfs_ws_create", "nwg_msbfs_ws_destroy",
     "nwg_msbfs", "nwg_ragged_register", "nwg_ragged_release", "nwg_ragged_info", "nwg_ragged_bfs",
     "nwg_server_create", "nwg_server_destroy", "nwg_server_submit", "nwg_server_wait", "nwg_server_run_trace",
-    "nwg_verify", "nwg_graph_read", "nwg_graph_write_nwbin",
+    "nwg_verify", "nwg_graph_read", "nwg_graph_write_nwbin", "nwg_bc",
 )
 
 
@@ -130,6 +130,10 @@ class VerifyResult(C.Structure):
                4: "reachability mismatch"}
 
 
+class BcStats(C.Structure):
+    _fields_ = [("sources", C.c_uint32), ("lanes", C.c_uint32), ("max_levels", C.c_uint32), ("device_ms", C.c_float)]
+
+
 _vp = C.c_void_p
 _u32, _u64, _int = C.c_uint32, C.c_uint64, C.c_int
 
@@ -174,6 +178,7 @@ def _load():
         "nwg_verify": (_int, [_vp, _u32, _vp, _vp, C.POINTER(VerifyResult)]),
         "nwg_graph_read": (_int, [C.c_char_p, _u32, C.POINTER(_vp)]),
         "nwg_graph_write_nwbin": (_int, [_vp, C.c_char_p]),
+        "nwg_bc": (_int, [_vp, _vp, _u32, _int, _u32, _vp, _vp, C.POINTER(BcStats)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -567,6 +572,17 @@ def depths_from_parents(parents: np.ndarray, root: int) -> np.ndarray:
         pending = pending[~ready]
         d += 1
     return depth
+
+
+def betweenness(g: Graph, sources, normalize: bool = True, lanes: int = 0):
+    """brandes_bc<float, double>(graph, sources, ...) on the GPU: (scores as
+    a host float32 array, BcStats)."""
+    src = np.ascontiguousarray(sources, dtype=np.uint32)
+    out = np.zeros(g.n, np.float32)
+    st = BcStats()
+    check(lib.nwg_bc(g.h, src.ctypes.data, src.size, 1 if normalize else 0, int(lanes), out.ctypes.data, None,
+                     C.byref(st)))
+    return out, st
 
 
 def verify(g: Graph, root: int, parents) -> VerifyResult:

@@ -17,6 +17,13 @@
  *                       depth[root] = 0, depth[v] = depth[parent[v]] + 1.
  *   nwgport_msbfs_depths  uint8 depths for a list of sources, each an
  *                       independent single-source BFS (255 = unreached).
+ *   nwgport_bc          approximate betweenness centrality over a list of
+ *                       sources, the computation of BCVerifier<float, double>
+ *                       (include/nwgraph/algorithms/betweenness_centrality.hpp:
+ *                       59-115): per source a serial BFS with double path
+ *                       counts, then float deltas accumulated from the deepest
+ *                       level up; every reached vertex, the source included,
+ *                       adds its delta; optional division by the largest score.
  *
  * The pow2(ceil_log2(num_bins)) bin count and the `u % n` binning of
  * bfs.hpp:166,181,287 only order the serial work here; they cannot change
@@ -297,4 +304,71 @@ int64_t nwgport_msbfs_depths(const uint64_t* off, const uint32_t* col, uint64_t 
   }
   free(d);
   return maxd;
+}
+
+
+/* Approximate betweenness centrality, BCVerifier's own computation
+ * (betweenness_centrality.hpp:63-115).  scores: n floats.  Returns 0, or -2
+ * when out of memory. */
+int64_t nwgport_bc(const uint64_t* off, const uint32_t* col, uint64_t N, const uint32_t* sources, uint32_t k,
+                   int normalize, float* scores) {
+  int32_t*  depth = (int32_t*)malloc(sizeof(int32_t) * (N ? N : 1));
+  double*   pc    = (double*)malloc(sizeof(double) * (N + 1));
+  float*    delta = (float*)malloc(sizeof(float) * (N ? N : 1));
+  uint32_t* order = (uint32_t*)malloc(sizeof(uint32_t) * (N ? N : 1));
+  uint64_t* lvl   = (uint64_t*)malloc(sizeof(uint64_t) * (N + 2));
+  if (!depth || !pc || !delta || !order || !lvl) {
+    free(depth), free(pc), free(delta), free(order), free(lvl);
+    return -2;
+  }
+  for (uint64_t i = 0; i < N; ++i) scores[i] = 0.0f;
+  for (uint32_t si = 0; si < k; ++si) {
+    const uint32_t s = sources[si];
+    for (uint64_t i = 0; i < N; ++i) {
+      depth[i] = -1;
+      pc[i]    = 0.0;
+      delta[i] = 0.0f;
+    }
+    depth[s] = 0;
+    pc[s]    = 1.0;
+    uint64_t head = 0, tail = 0;
+    order[tail++] = s;
+    /* forward: BFS order with path counts (:66-83) */
+    while (head < tail) {
+      const uint32_t u = order[head++];
+      for (uint64_t e = off[u]; e < off[u + 1]; ++e) {
+        const uint32_t v = col[e];
+        if (depth[v] == -1) {
+          depth[v]      = depth[u] + 1;
+          order[tail++] = v;
+        }
+        if (depth[v] == depth[u] + 1) pc[v] += pc[u];
+      }
+    }
+    /* levels in BFS order are contiguous: lvl[d] = first index of depth d */
+    uint64_t nlev = 0;
+    for (uint64_t i = 0; i < tail; ++i)
+      if (i == 0 || depth[order[i]] != depth[order[i - 1]]) lvl[nlev++] = i;
+    lvl[nlev] = tail;
+    /* backward, deepest level first (:96-107); within a level the vertices
+     * are independent, so their order does not change any value */
+    for (int64_t d = (int64_t)nlev - 1; d >= 0; --d) {
+      for (uint64_t i = lvl[d]; i < lvl[d + 1]; ++i) {
+        const uint32_t u = order[i];
+        for (uint64_t e = off[u]; e < off[u + 1]; ++e) {
+          const uint32_t v = col[e];
+          if (depth[v] == depth[u] + 1) delta[u] += pc[u] / pc[v] * (1 + delta[v]);
+        }
+        scores[u] += delta[u];
+      }
+    }
+  }
+  if (normalize && N) {
+    float big = scores[0];
+    for (uint64_t i = 1; i < N; ++i)
+      if (scores[i] > big) big = scores[i];
+    for (uint64_t i = 0; i < N; ++i) scores[i] = scores[i] / big;
+  }
+  free(depth), free(pc), free(delta), free(order), free(lvl);
+  return 0;
 }

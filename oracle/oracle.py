@@ -28,6 +28,7 @@ NULLV = 0xFFFFFFFF
 _u64p = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
 _u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
 _u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+_f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 
 
 def build_port(force: bool = False) -> str:
@@ -103,6 +104,8 @@ class Port:
         lib.nwgport_depths_from_parents.argtypes = [_u32p, C.c_uint64, C.c_uint32, _u32p]
         lib.nwgport_verify.restype = C.c_int
         lib.nwgport_verify.argtypes = [_u64p, _u32p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32, _u32p]
+        lib.nwgport_bc.restype = C.c_int64
+        lib.nwgport_bc.argtypes = [_u64p, _u32p, C.c_uint64, _u32p, C.c_uint32, C.c_int, _f32p]
         lib.nwgport_msbfs_depths.restype = C.c_int64
         lib.nwgport_msbfs_depths.argtypes = [_u64p, _u32p, C.c_uint64, _u32p, C.c_uint32, _u8p]
         self.lib = lib
@@ -150,6 +153,14 @@ class Port:
         return self.lib.nwgport_verify(off, cols, io, ic, off.size - 1, int(root),
                                        np.ascontiguousarray(parents, np.uint32)) == 1
 
+    def bc(self, off, cols, sources, normalize=True):
+        """BCVerifier's approximate betweenness centrality (float scores)."""
+        src = np.ascontiguousarray(sources, np.uint32)
+        out = np.zeros(off.size - 1, np.float32)
+        if self.lib.nwgport_bc(off, cols, off.size - 1, src, src.size, 1 if normalize else 0, out) < 0:
+            raise MemoryError("nwgport_bc")
+        return out
+
     def msbfs_depths(self, off, cols, roots):
         roots = np.ascontiguousarray(roots, np.uint32)
         out = np.empty((roots.size, off.size - 1), np.uint8)
@@ -178,6 +189,10 @@ class Reference:
         lib.nwgref_bfs_serial.argtypes = [C.c_void_p, C.c_uint32, _u32p]
         lib.nwgref_verify.restype = C.c_int
         lib.nwgref_verify.argtypes = [C.c_void_p, C.c_uint32, _u32p, C.c_uint64]
+        lib.nwgref_bc.restype = C.c_int
+        lib.nwgref_bc.argtypes = [C.c_void_p, _u32p, C.c_uint64, C.c_int, C.c_int, _f32p, C.POINTER(C.c_double)]
+        lib.nwgref_bc_verify.restype = C.c_int
+        lib.nwgref_bc_verify.argtypes = [C.c_void_p, _u32p, C.c_uint64, _f32p, C.c_uint64]
         lib.nwgref_threads.restype = C.c_int
         lib.nwgref_set_threads.argtypes = [C.c_int]
         self.lib = lib
@@ -212,6 +227,20 @@ class Reference:
         def verify(self, root, parents):
             return self.ref.lib.nwgref_verify(self.h, int(root), np.ascontiguousarray(parents, np.uint32),
                                               self.n) == 1
+
+        def bc(self, sources, threads=0, normalize=True):
+            """brandes_bc<float, double>(out, sources, threads): (scores, seconds)."""
+            src = np.ascontiguousarray(sources, np.uint32)
+            out = np.zeros(self.n, np.float32)
+            secs = C.c_double()
+            t = int(threads) if threads else self.ref.threads()
+            self.ref.lib.nwgref_bc(self.h, src, src.size, t, 1 if normalize else 0, out, C.byref(secs))
+            return out, secs.value
+
+        def bc_verify(self, sources, scores):
+            src = np.ascontiguousarray(sources, np.uint32)
+            return bool(self.ref.lib.nwgref_bc_verify(self.h, src, src.size, np.ascontiguousarray(scores, np.float32),
+                                                      self.n))
 
         def close(self):
             if self.h:

@@ -16,12 +16,19 @@
 //   nwgref_bfs_serial    - nw::graph::bfs(graph, root) (algorithms/bfs.hpp:110-140)
 //   nwgref_verify        - BFSVerifier(out, in, root, parents)
 //                          (algorithms/bfs.hpp:44-98)
+//   nwgref_bc            - brandes_bc<float, double>(out, sources, threads)
+//                          (algorithms/betweenness_centrality.hpp:218-324),
+//                          the parallel approximate betweenness centrality
+//                          NWGraph's bench/bc.cpp:136 runs, timed with a wall clock
+//   nwgref_bc_verify     - BCVerifier<float, double>(out, sources, scores)
+//                          (algorithms/betweenness_centrality.hpp:59-128)
 #include <chrono>
 #include <cstdint>
 #include <cstring>
 #include <vector>
 
 #include "nwgraph/adjacency.hpp"
+#include "nwgraph/algorithms/betweenness_centrality.hpp"
 #include "nwgraph/algorithms/bfs.hpp"
 
 #define NWGREF_API extern "C" __attribute__((visibility("default")))
@@ -80,6 +87,26 @@ NWGREF_API int nwgref_verify(void* h, uint32_t root, const uint32_t* parents, ui
   auto*                 p = static_cast<ref_pair*>(h);
   std::vector<uint32_t> par(parents, parents + n);
   return nw::graph::BFSVerifier(p->out, *p->in, root, par) ? 1 : 0;
+}
+
+NWGREF_API int nwgref_bc(void* h, const uint32_t* sources, uint64_t k, int threads, int normalize, float* scores_out,
+                         double* seconds_out) {
+  auto*                 p = static_cast<ref_pair*>(h);
+  std::vector<uint32_t> src(sources, sources + k);
+  auto                  start = std::chrono::high_resolution_clock::now();
+  auto sc = nw::graph::brandes_bc<float, double>(p->out, src, threads, std::execution::par_unseq, std::execution::par_unseq,
+                                                 normalize != 0);
+  std::chrono::duration<double> el = std::chrono::high_resolution_clock::now() - start;
+  if (seconds_out) *seconds_out = el.count();
+  std::memcpy(scores_out, sc.data(), sc.size() * sizeof(float));
+  return 0;
+}
+
+NWGREF_API int nwgref_bc_verify(void* h, const uint32_t* sources, uint64_t k, const float* scores, uint64_t n) {
+  auto*                 p = static_cast<ref_pair*>(h);
+  std::vector<uint32_t> src(sources, sources + k);
+  std::vector<float>    sc(scores, scores + n);
+  return nw::graph::BCVerifier<float, double>(p->out, src, sc) ? 1 : 0;
 }
 
 NWGREF_API int nwgref_threads() { return tbb::this_task_arena::max_concurrency(); }

@@ -454,6 +454,42 @@ class global_control {
   long      prev_ = 0;
 };
 
+// A priority queue behind one mutex (top = greatest under Compare).
+template <class T, class Compare = std::less<T>>
+class concurrent_priority_queue {
+ public:
+  void push(const T& v) {
+    std::lock_guard<std::mutex> lk(mu_);
+    h_.push_back(v);
+    std::push_heap(h_.begin(), h_.end(), cmp_);
+  }
+  bool try_pop(T& out) {
+    std::lock_guard<std::mutex> lk(mu_);
+    if (h_.empty()) return false;
+    std::pop_heap(h_.begin(), h_.end(), cmp_);
+    out = h_.back();
+    h_.pop_back();
+    return true;
+  }
+  bool empty() const {
+    std::lock_guard<std::mutex> lk(mu_);
+    return h_.empty();
+  }
+  std::size_t size() const {
+    std::lock_guard<std::mutex> lk(mu_);
+    return h_.size();
+  }
+  void clear() {
+    std::lock_guard<std::mutex> lk(mu_);
+    h_.clear();
+  }
+
+ private:
+  mutable std::mutex mu_;
+  std::vector<T>     h_;
+  Compare            cmp_;
+};
+
 namespace this_task_arena {
 inline int max_concurrency() { return (int)detail_compat::active_threads(); }
 }  // namespace this_task_arena

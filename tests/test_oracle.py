@@ -229,3 +229,29 @@ def test_nwbin_fixtures_follow_the_reference_layout(golden):
             assert np.array_equal(off, G.off)
             rows = [np.sort(cols[off[u]:off[u + 1]]) for u in range(vcount)]
             assert np.array_equal(np.concatenate(rows), G.cols)
+
+
+def test_bc_restatement_matches_reference(port, reference):
+    """nwgport_bc restates BCVerifier's computation; NWGraph's parallel
+    brandes_bc<float, double> and its BCVerifier agree with it."""
+    if reference is None:
+        pytest.skip("reference oracle not built here")
+    for scale, seed in ((10, 1), (12, 2)):
+        off, cols = gg.rmat(scale, 16, seed=seed)
+        src = gg.roots(off, 8, seed=3)
+        mine = port.bc(off, cols, src)
+        g = reference.graph(off, cols)
+        theirs, secs = g.bc(src)
+        assert secs > 0
+        assert np.max(np.abs(mine - theirs)) <= 1e-6
+        assert g.bc_verify(src, mine) and g.bc_verify(src, theirs)
+        # errors planted in the oracle's scores: the reference's BCVerifier
+        # takes abs() of a float difference through the integer overload
+        # (betweenness_centrality.hpp:119), so it misses anything below 1;
+        # the tests here compare |difference| <= 1e-6 themselves
+        bad = mine.copy()
+        bad[int(np.argmax(mine))] -= 1e-3
+        assert g.bc_verify(src, bad) and np.max(np.abs(bad - theirs)) > 1e-6
+        bad[int(np.argmax(mine))] += 2.0
+        assert not g.bc_verify(src, bad)
+        g.close()
