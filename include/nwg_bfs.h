@@ -131,6 +131,16 @@ int nwg_bfs_stepped(nwg_graph g, uint32_t root, int alpha, int beta, uint32_t* p
  * nw::graph::bfs(graph, root) (algorithms/bfs.hpp:110-140). */
 int nwg_bfs_topdown(nwg_graph g, uint32_t root, uint32_t* parents_host, uint32_t* parents_dev, nwg_bfs_stats* stats);
 
+/* Failure-detection self-test (no reference counterpart).  Runs the
+ * persistent small-frontier kernel's grid barrier on a grid that never
+ * completes it (a wait for one block more than the grid has): every block
+ * gives up after `spins` polls (1..2^24; each poll sleeps about 32 ns plus an
+ * L2 round trip) and reports NWG_ETIMEDOUT, the status a traversal returns
+ * when a block never arrives.  status receives that device-side status,
+ * waited_ms the device time.  No fault, trap or unbounded wait is involved;
+ * the context stays usable. */
+int nwg_selftest_wait_timeout(uint32_t spins, int32_t* status, float* waited_ms);
+
 /* Sum of out-degrees and count of the vertices reached in a device parents
  * array (the TEPS numerator of a traversal); both outputs may be NULL. */
 int nwg_component_edges(nwg_graph g, const uint32_t* parents_dev, uint64_t* edges, uint64_t* vertices);

@@ -41,7 +41,7 @@ EXPORTED = (
     "nwg_gen_grid", "nwg_pick_roots", "nwg_bfs_noalloc", "nwg_msbfs_ws_create", "nwg_msbfs_ws_destroy",
     "nwg_msbfs", "nwg_ragged_register", "nwg_ragged_release", "nwg_ragged_info", "nwg_ragged_bfs",
     "nwg_server_create", "nwg_server_destroy", "nwg_server_submit", "nwg_server_wait", "nwg_server_run_trace",
-    "nwg_verify", "nwg_graph_read", "nwg_graph_write_nwbin", "nwg_bc",
+    "nwg_verify", "nwg_graph_read", "nwg_graph_write_nwbin", "nwg_bc", "nwg_selftest_wait_timeout",
 )
 
 
@@ -179,6 +179,7 @@ def _load():
         "nwg_graph_read": (_int, [C.c_char_p, _u32, C.POINTER(_vp)]),
         "nwg_graph_write_nwbin": (_int, [_vp, C.c_char_p]),
         "nwg_bc": (_int, [_vp, _vp, _u32, _int, _u32, _vp, _vp, C.POINTER(BcStats)]),
+        "nwg_selftest_wait_timeout": (_int, [_u32, C.POINTER(C.c_int32), C.POINTER(C.c_float)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -470,6 +470,14 @@ NWG_API int nwg_msbfs(nwg_msbfs_ws h, const uint32_t* roots_host, uint32_t k, ui
   NWG_GUARD_END
 }
 
+NWG_API int nwg_selftest_wait_timeout(uint32_t spins, int32_t* status, float* waited_ms) {
+  NWG_GUARD_BEGIN
+  if (!status || !waited_ms) return set_error(NWG_EINVAL, "NULL argument");
+  if (spins == 0 || spins > (1u << 24)) return set_error(NWG_EINVAL, "spins must be 1..2^24");
+  return wait_probe(spins, status, waited_ms);
+  NWG_GUARD_END
+}
+
 NWG_API int nwg_component_edges(nwg_graph h, const uint32_t* parents_dev, uint64_t* edges, uint64_t* vertices) {
   NWG_GUARD_BEGIN
   if (!h || !parents_dev) return set_error(NWG_EINVAL, "NULL argument");

@@ -802,7 +802,7 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned* a) {
   return v;
 }
 
-__device__ __forceinline__ bool grid_barrier(const DobfsParams& p, unsigned nblocks) {
+__device__ __forceinline__ bool grid_barrier(const DobfsParams& p, unsigned nblocks, unsigned max_spins = kBarrierSpins) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -818,7 +818,7 @@ __device__ __forceinline__ bool grid_barrier(const DobfsParams& p, unsigned nblo
       } else {
         unsigned spins = 0;
         while (ld_acquire(&bar->gen) == g) {
-          if (++spins > kBarrierSpins) {
+          if (++spins > max_spins) {
             atomicCAS(&p.ctrl->err, 0, NWG_ETIMEDOUT);
             ok = 0;
             break;
@@ -1562,6 +1562,47 @@ int ragged_launch(RaggedDev* r, uint32_t n_items, uint32_t* parents_dev, uint32_
   NWG_CUDA_TRY(cudaEventRecord(r->ev1, r->stream));
   NWG_CUDA_TRY(cudaEventSynchronize(r->ev1));
   if (ms) cudaEventElapsedTime(ms, r->ev0, r->ev1);
+  return NWG_OK;
+}
+
+// Failure-detection probe: the persistent kernel's grid barrier, waited on
+// for one more block than the grid has, so no one ever releases it.  Every
+// block gives up after max_spins polls, records NWG_ETIMEDOUT and returns --
+// the path a real barrier takes when a block never arrives.
+__global__ void k_wait_probe(DobfsParams p, unsigned max_spins) {
+  const bool ok = grid_barrier(p, gridDim.x + 1, max_spins);
+  if (!ok && threadIdx.x == 0 && blockIdx.x == 0) p.ctrl->h.status = __ldcg(&p.ctrl->err);
+}
+
+int wait_probe(uint32_t spins, int32_t* status, float* waited_ms) {
+  Ctrl* ctrl = nullptr;
+  if (cudaMalloc(&ctrl, sizeof(Ctrl)) != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(NWG_ENOMEM, "probe control block");
+  }
+  DobfsParams p = {};
+  p.ctrl        = ctrl;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaError_t e  = cudaMemset(ctrl, 0, sizeof(Ctrl));
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  if (e == cudaSuccess) e = cudaEventRecord(e0, 0);
+  if (e == cudaSuccess) {
+    k_wait_probe<<<2, kThreads, 0, 0>>>(p, spins);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(e1, 0);
+  if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+  int32_t st = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(&st, &ctrl->h.status, sizeof st, cudaMemcpyDeviceToHost);
+  float ms = 0.f;
+  if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(ctrl);
+  if (e != cudaSuccess) return cuda_error(e, "wait probe");
+  *status    = st;
+  *waited_ms = ms;
   return NWG_OK;
 }
 

@@ -265,6 +265,7 @@ int         cuda_error(cudaError_t e, const char* what);
   } while (0)
 
 // nwg_dobfs.cu
+int  wait_probe(uint32_t spins, int32_t* status, float* waited_ms);
 int  ws_init(GraphDev* g, Workspace* ws);
 void ws_free(Workspace* ws);
 int  ws_launch(Workspace* ws, uint32_t root, int alpha, int beta, uint32_t* parents, cudaStream_t stream,
