@@ -75,6 +75,11 @@ def parse():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-verify", action="store_true")
     ap.add_argument("--no-bc", action="store_true")
+    ap.add_argument("--profile-msbfs", action="store_true",
+                    help="one 64-source multi-source pass on RMAT-22, levels driven from the host, in NVTX range "
+                         "nwg_profile (for ncu)")
+    ap.add_argument("--profile-bc", action="store_true",
+                    help="betweenness from one source on RMAT-22 in NVTX range nwg_profile (for ncu)")
     ap.add_argument("--serve-slots", type=int, default=16)
     ap.add_argument("--profile-one", action="store_true",
                     help="after warm-up, run one traversal inside an NVTX range 'nwg_profile' and exit (for ncu)")
@@ -341,6 +346,36 @@ def bench_ragged(nwg, torch, num_graphs=1000, reps=3):
             "classes": {k: v.__dict__ for k, v in params.items()}, "generate_s": gen_s, "autotune_s": tune_s}
 
 
+def profile_extension(args, torch):
+    """Single runs of the multi-source pass or of betweenness for a profiler."""
+    if args.profile_msbfs:
+        os.environ["NWG_MS_STEPPED"] = "1"  # kernels launched one by one (ncu cannot enter conditional graphs)
+    import nwgr_b200 as nwg
+
+    g = nwg.Graph.rmat(22, 16, seed=GRAPH_SEED)
+    roots = g.roots(64, seed=ROOT_SEED)
+    if args.profile_msbfs:
+        ws = nwg.MsWorkspace(g)
+        depths = torch.empty((64, g.n), dtype=torch.uint8, device="cuda")
+        ws.run(roots, depths)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("nwg_profile")
+        st = ws.run(roots, depths)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
+        print(json.dumps({"profile_msbfs": True, "levels": st.levels, "push": st.push_levels, "pull": st.pull_levels}))
+        ws.close()
+    else:
+        nwg.betweenness(g, roots[:1], lanes=1)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("nwg_profile")
+        _, st = nwg.betweenness(g, roots[:1], lanes=1)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
+        print(json.dumps({"profile_bc": True, "levels": st.max_levels, "device_ms": st.device_ms}))
+    g.release()
+
+
 def bench_verifier(nwg, torch, g, roots, with_cpu):
     """Device BFSVerifier (nwg_verify) on the bench graph: device time of the
     check (its own top-down BFS plus the per-vertex parent checks) for the
@@ -470,6 +505,9 @@ def main():
         return
 
     torch.cuda.set_device(local)
+    if args.profile_msbfs or args.profile_bc:
+        profile_extension(args, torch)
+        return
     dist = None
     if world > 1:
         import datetime

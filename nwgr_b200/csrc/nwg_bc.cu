@@ -22,7 +22,9 @@
 // claims levels with atomicCAS and adds path counts with double atomics
 // (integers: exact below 2^53, so the order of the adds does not matter);
 // the backward phase sums a task's terms with a warp reduction and adds one
-// double per task.  Several sources run at once, one host thread and stream
+// double per task.
+// Every vertex's level, dependency and path count (or, once its dependency
+// is final, its weight) share one 16-byte record.  Several sources run at once, one host thread and stream
 // each.  Scores are float sums across sources, as in the reference.
 #include <algorithm>
 #include <atomic>
@@ -43,9 +45,17 @@ constexpr int      kBcThreads = 256;
 constexpr uint32_t kBcTask    = 2048;  // out-edges per warp task
 constexpr uint32_t kUnset     = 0xFFFFFFFFu;
 
+// Per-vertex state of one source, one 16-byte record so that a backward
+// edge reads its target's level, dependency and path count in one sector.
+struct alignas(16) BcVertex {
+  uint32_t level;  // BFS level (kUnset = unreached)
+  float    delta;  // dependency (score_t)
+  double   sigma;  // shortest-path count (accum_t)
+};
+
 struct BcCounters {
-  unsigned long long next;   // vertices appended to the next level
-  unsigned int       tasks;  // tasks of the current level
+  unsigned long long next;      // vertices appended to the next level
+  unsigned int       tasks;     // out-edge tasks of the current level
   unsigned int       pad;
 };
 
@@ -59,10 +69,12 @@ __global__ void k_bc_tasks(const uint64_t* __restrict__ off, const uint32_t* __r
   }
 }
 
-// total = last exclusive prefix + last count.
-__global__ void k_bc_total(const uint32_t* tpre, const uint32_t* tasks, uint64_t count, BcCounters* cnt) {
-  cnt->tasks = count ? tpre[count - 1] + tasks[count - 1] : 0u;
-  cnt->next  = 0;
+// total = last exclusive prefix + last count (into *total); the claim pass
+// also restarts the next-level counter.
+__global__ void k_bc_total(const uint32_t* tpre, const uint32_t* tasks, uint64_t count, unsigned int* total,
+                           unsigned long long* next) {
+  *total = count ? tpre[count - 1] + tasks[count - 1] : 0u;
+  if (next) *next = 0;
 }
 
 // Owner of task t: the last i with tpre[i] <= t.
@@ -77,8 +89,8 @@ __device__ __forceinline__ uint64_t task_owner(const uint32_t* tpre, uint64_t co
 }
 
 __global__ void __launch_bounds__(kBcThreads) k_bc_forward(const uint64_t* __restrict__ off,
-                                                           const uint32_t* __restrict__ col, uint32_t* level,
-                                                           double* sigma, const uint32_t* __restrict__ order,
+                                                           const uint32_t* __restrict__ col, BcVertex* vx,
+                                                           const uint32_t* __restrict__ order,
                                                            const uint32_t* __restrict__ tpre, uint64_t count,
                                                            uint32_t* next, uint64_t next_cap, uint32_t lvl,
                                                            BcCounters* cnt) {
@@ -89,7 +101,7 @@ __global__ void __launch_bounds__(kBcThreads) k_bc_forward(const uint64_t* __res
   for (uint64_t t = gwarp; t < ntask; t += nwarps) {
     const uint64_t i   = task_owner(tpre, count, (uint32_t)t);
     const uint32_t u   = order[i];
-    const double   su  = sigma[u];
+    const double   su  = vx[u].sigma;
     const uint64_t beg = off[u] + (uint64_t)((uint32_t)t - tpre[i]) * kBcTask;
     const uint64_t end = min(off[u + 1], beg + kBcTask);
     for (uint64_t e0 = beg; e0 < end; e0 += 32) {
@@ -98,13 +110,13 @@ __global__ void __launch_bounds__(kBcThreads) k_bc_forward(const uint64_t* __res
       uint32_t       v   = 0;
       if (e < end) {
         v           = col[e];
-        uint32_t lv = level[v];
+        uint32_t lv = vx[v].level;
         if (lv == kUnset) {
-          lv  = atomicCAS(&level[v], kUnset, lvl + 1);
+          lv  = atomicCAS(&vx[v].level, kUnset, lvl + 1);
           won = lv == kUnset;
           if (won) lv = lvl + 1;
         }
-        if (lv == lvl + 1) atomicAdd(&sigma[v], su);
+        if (lv == lvl + 1) atomicAdd(&vx[v].sigma, su);  // same 16-byte record as the level
       }
       const unsigned m = __ballot_sync(kFullMask, won);
       if (m) {
@@ -120,11 +132,9 @@ __global__ void __launch_bounds__(kBcThreads) k_bc_forward(const uint64_t* __res
   }
 }
 
-__global__ void __launch_bounds__(kBcThreads) k_bc_backward(const uint64_t* __restrict__ off,
+__global__ void __launch_bounds__(kBcThreads, 4) k_bc_backward(const uint64_t* __restrict__ off,
                                                             const uint32_t* __restrict__ col,
-                                                            const uint32_t* __restrict__ level,
-                                                            const double* __restrict__ sigma,
-                                                            const float* __restrict__ delta, double* dsum,
+                                                            const BcVertex* __restrict__ vx, double* dsum,
                                                             const uint32_t* __restrict__ order,
                                                             const uint32_t* __restrict__ tpre, uint64_t count,
                                                             uint32_t ntask, uint32_t lvl) {
@@ -134,13 +144,13 @@ __global__ void __launch_bounds__(kBcThreads) k_bc_backward(const uint64_t* __re
   for (uint64_t t = gwarp; t < ntask; t += nwarps) {
     const uint64_t i   = task_owner(tpre, count, (uint32_t)t);
     const uint32_t u   = order[i];
-    const double   su  = sigma[u];
+    const double   su  = vx[u].sigma;
     const uint64_t beg = off[u] + (uint64_t)((uint32_t)t - tpre[i]) * kBcTask;
     const uint64_t end = min(off[u + 1], beg + kBcTask);
     double         acc = 0.0;
     for (uint64_t e = beg + lane; e < end; e += 32) {
-      const uint32_t v = col[e];
-      if (level[v] == lvl + 1) acc += su / sigma[v] * (double)(1.0f + delta[v]);
+      const BcVertex r = vx[col[e]];  // level and weight in one 16-byte load
+      if (r.level == lvl + 1) acc += su * r.sigma;  // r.sigma holds (1 + delta[v]) / path_counts[v] by now
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(kFullMask, acc, o);
@@ -148,23 +158,30 @@ __global__ void __launch_bounds__(kBcThreads) k_bc_backward(const uint64_t* __re
   }
 }
 
-// delta[u] = the level's sums as float; bc[u] += delta[u].
-__global__ void k_bc_finish(const uint32_t* __restrict__ order, uint64_t count, double* dsum, float* delta,
+// delta[u] = the level's sums as float; bc[u] += delta[u].  The path count
+// of u is not needed any more (u's own sum is done), so its slot takes the
+// weight (1 + delta[u]) / path_counts[u] that the level above multiplies by:
+// the reference's path_counts[w] / path_counts[u] * (1.0f + deltas[u])
+// (:301) with the division done once per vertex instead of once per edge.
+__global__ void k_bc_finish(const uint32_t* __restrict__ order, uint64_t count, double* dsum, BcVertex* vx,
                             float* bc) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
     const uint32_t u = order[i];
     const float    d = (float)dsum[u];
-    delta[u]         = d;
+    vx[u].delta      = d;
+    vx[u].sigma      = (double)(1.0f + d) / vx[u].sigma;
     dsum[u]          = 0.0;
     atomicAdd(&bc[u], d);
   }
 }
 
-__global__ void k_bc_root(uint32_t* level, double* sigma, uint32_t* order, uint32_t s) {
-  level[s] = 0;
-  sigma[s] = 1.0;
-  order[0] = s;
+// Every vertex unreached, no path, no dependency; then the source.
+__global__ void k_bc_reset(BcVertex* vx, uint64_t n, uint32_t* order, uint32_t s) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    vx[i] = (i == s) ? BcVertex{0u, 0.0f, 1.0} : BcVertex{kUnset, 0.0f, 0.0};
+  if (blockIdx.x == 0 && threadIdx.x == 0) order[0] = s;
 }
 
 // Largest score (non-negative floats: their bit patterns order as integers).
@@ -184,18 +201,23 @@ __global__ void k_bc_divide(float* bc, uint64_t n, const unsigned int* maxbits) 
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) bc[i] = bc[i] / big;
 }
 
-int grid_bc(const GraphDev* g, uint64_t items, uint64_t per_block) {
+// Grid of a grid-stride kernel: no more blocks than fit on the GPU at once
+// (the tasks are dealt out statically, so blocks of a second wave would
+// start only when the first wave ends), and no more than the work needs.
+template <class K>
+int grid_bc(const GraphDev* g, K kernel, uint64_t items, uint64_t per_block) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBcThreads, 0) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
   const uint64_t want = (items + per_block - 1) / per_block;
-  return (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)g->sm_count * 8, want));
+  return (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)g->sm_count * per_sm, want));
 }
 
 // One concurrent source lane: its stream and per-vertex state.
 struct BcSlot {
   cudaStream_t s     = nullptr;
-  uint32_t*    level = nullptr;
-  double*      sigma = nullptr;
+  BcVertex*    vx    = nullptr;
   double*      dsum  = nullptr;
-  float*       delta = nullptr;
   uint32_t*    order = nullptr;
   uint32_t*    tasks = nullptr;
   uint32_t*    tpre  = nullptr;
@@ -210,10 +232,8 @@ struct BcSlot {
 
 void slot_free(BcSlot& b) {
   if (b.s) cudaStreamSynchronize(b.s);
-  cudaFree(b.level);
-  cudaFree(b.sigma);
+  cudaFree(b.vx);
   cudaFree(b.dsum);
-  cudaFree(b.delta);
   cudaFree(b.order);
   cudaFree(b.tasks);
   cudaFree(b.tpre);
@@ -225,8 +245,7 @@ void slot_free(BcSlot& b) {
 
 int slot_init(const GraphDev* g, BcSlot& b) {
   const uint64_t n = std::max<uint64_t>(g->n, 1);
-  if (cudaMalloc(&b.level, n * 4) != cudaSuccess || cudaMalloc(&b.sigma, n * 8) != cudaSuccess ||
-      cudaMalloc(&b.dsum, n * 8) != cudaSuccess || cudaMalloc(&b.delta, n * 4) != cudaSuccess ||
+  if (cudaMalloc(&b.vx, n * sizeof(BcVertex)) != cudaSuccess || cudaMalloc(&b.dsum, n * 8) != cudaSuccess ||
       cudaMalloc(&b.order, n * 4) != cudaSuccess || cudaMalloc(&b.tasks, n * 4) != cudaSuccess ||
       cudaMalloc(&b.tpre, n * 4) != cudaSuccess || cudaMalloc(&b.cnt, sizeof(BcCounters)) != cudaSuccess ||
       cudaMallocHost(&b.hcnt, sizeof(BcCounters)) != cudaSuccess) {
@@ -248,20 +267,18 @@ int slot_init(const GraphDev* g, BcSlot& b) {
 int run_source(const GraphDev* g, BcSlot& b, uint32_t s, float* bc) {
   const uint64_t n = g->n;
   cudaStream_t   st = b.s;
-  NWG_CUDA_TRY(cudaMemsetAsync(b.level, 0xFF, n * 4, st));
-  NWG_CUDA_TRY(cudaMemsetAsync(b.sigma, 0, n * 8, st));
-  k_bc_root<<<1, 1, 0, st>>>(b.level, b.sigma, b.order, s);
+  k_bc_reset<<<grid_bc(g, k_bc_reset, n, kBcThreads), kBcThreads, 0, st>>>(b.vx, n, b.order, s);
   std::vector<uint64_t> lo = {0, 1};  // level L = order[lo[L], lo[L + 1])
   std::vector<uint32_t> ntask;         // tasks of each level (kept for the backward pass)
   for (uint32_t L = 0;; ++L) {
     const uint64_t count = lo[L + 1] - lo[L];
     const uint32_t* lv   = b.order + lo[L];
-    k_bc_tasks<<<grid_bc(g, count, kBcThreads), kBcThreads, 0, st>>>(g->off, lv, count, b.tasks + lo[L]);
+    k_bc_tasks<<<grid_bc(g, k_bc_tasks, count, kBcThreads), kBcThreads, 0, st>>>(g->off, lv, count, b.tasks + lo[L]);
     NWG_CUDA_TRY(cub::DeviceScan::ExclusiveSum(b.tmp, b.tmp_bytes, b.tasks + lo[L], b.tpre + lo[L], (int64_t)count, st));
-    k_bc_total<<<1, 1, 0, st>>>(b.tpre + lo[L], b.tasks + lo[L], count, b.cnt);
-    // a task covers at most kBcTask edges: the grid is sized by the level's edges
-    k_bc_forward<<<grid_bc(g, g->m / kBcTask + count, kBcThreads / 32), kBcThreads, 0, st>>>(
-        g->off, g->col, b.level, b.sigma, lv, b.tpre + lo[L], count, b.order + lo[L + 1], n - lo[L + 1], L, b.cnt);
+    k_bc_total<<<1, 1, 0, st>>>(b.tpre + lo[L], b.tasks + lo[L], count, &b.cnt->tasks, &b.cnt->next);
+    // claims: a task covers at most kBcTask edges, the grid is sized by the level's edges
+    k_bc_forward<<<grid_bc(g, k_bc_forward, g->m / kBcTask + count, kBcThreads / 32), kBcThreads, 0, st>>>(
+        g->off, g->col, b.vx, lv, b.tpre + lo[L], count, b.order + lo[L + 1], n - lo[L + 1], L, b.cnt);
     NWG_CUDA_TRY(cudaGetLastError());
     NWG_CUDA_TRY(cudaMemcpyAsync(b.hcnt, b.cnt, sizeof(BcCounters), cudaMemcpyDeviceToHost, st));
     NWG_CUDA_TRY(cudaStreamSynchronize(st));
@@ -276,9 +293,9 @@ int run_source(const GraphDev* g, BcSlot& b, uint32_t s, float* bc) {
     const uint64_t count = lo[L + 1] - lo[L];
     const uint32_t nt    = ntask[L];  // the forward pass left the level's tpre in place
     if (nt)
-      k_bc_backward<<<grid_bc(g, nt, kBcThreads / 32), kBcThreads, 0, st>>>(
-          g->off, g->col, b.level, b.sigma, b.delta, b.dsum, b.order + lo[L], b.tpre + lo[L], count, nt, (uint32_t)L);
-    k_bc_finish<<<grid_bc(g, count, kBcThreads), kBcThreads, 0, st>>>(b.order + lo[L], count, b.dsum, b.delta, bc);
+      k_bc_backward<<<grid_bc(g, k_bc_backward, nt, kBcThreads / 32), kBcThreads, 0, st>>>(
+          g->off, g->col, b.vx, b.dsum, b.order + lo[L], b.tpre + lo[L], count, nt, (uint32_t)L);
+    k_bc_finish<<<grid_bc(g, k_bc_finish, count, kBcThreads), kBcThreads, 0, st>>>(b.order + lo[L], count, b.dsum, b.vx, bc);
     NWG_CUDA_TRY(cudaGetLastError());
   }
   NWG_CUDA_TRY(cudaStreamSynchronize(st));
@@ -336,21 +353,25 @@ NWG_API int nwg_bc(nwg_graph h, const uint32_t* sources, uint32_t k, int normali
     NWG_CUDA_TRY(cudaDeviceSynchronize());
     NWG_CUDA_TRY(cudaEventRecord(ev0, 0));
     if (!rc) {
-      std::atomic<uint32_t>    next{0};
-      std::vector<std::thread> th;
-      for (auto& b : slots)
-        th.emplace_back([&, dev = g->device](BcSlot* bp) {
-          cudaSetDevice(dev);
-          for (uint32_t i = next++; i < k && bp->rc == NWG_OK; i = next++) {
-            bp->rc = run_source(g, *bp, sources[i], bc);
-            if (bp->rc) {
-              char buf[512];
-              nwg_last_error(buf, sizeof buf);
-              bp->err = buf;
-            }
+      std::atomic<uint32_t> next{0};
+      auto                  lane_loop = [&, dev = g->device](BcSlot* bp) {
+        cudaSetDevice(dev);
+        for (uint32_t i = next++; i < k && bp->rc == NWG_OK; i = next++) {
+          bp->rc = run_source(g, *bp, sources[i], bc);
+          if (bp->rc) {
+            char buf[512];
+            nwg_last_error(buf, sizeof buf);
+            bp->err = buf;
           }
-        }, &b);
-      for (auto& t : th) t.join();
+        }
+      };
+      if (slots.size() == 1) {
+        lane_loop(&slots[0]);  // one lane: the calling thread (profiler ranges stay on it)
+      } else {
+        std::vector<std::thread> th;
+        for (auto& b : slots) th.emplace_back(lane_loop, &b);
+        for (auto& t : th) t.join();
+      }
       for (auto& b : slots)
         if (b.rc && !rc) {
           rc = b.rc;
@@ -358,8 +379,8 @@ NWG_API int nwg_bc(nwg_graph h, const uint32_t* sources, uint32_t k, int normali
         }
     }
     if (!rc && normalize) {
-      k_bc_max<<<grid_bc(g, n, 256), 256>>>(bc, n, maxbits);
-      k_bc_divide<<<grid_bc(g, n, 256), 256>>>(bc, n, maxbits);
+      k_bc_max<<<grid_bc(g, k_bc_max, n, 256), 256>>>(bc, n, maxbits);
+      k_bc_divide<<<grid_bc(g, k_bc_divide, n, 256), 256>>>(bc, n, maxbits);
       cudaError_t e = cudaGetLastError();
       if (e != cudaSuccess) rc = cuda_error(e, "betweenness normalisation");
     }

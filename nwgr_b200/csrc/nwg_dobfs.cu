@@ -1228,6 +1228,17 @@ __global__ void k_zero_indegree_packed(const uint64_t* __restrict__ off, const R
 
 int grid_for(const GraphDev* g, int per_sm) { return std::max(1, g->sm_count * per_sm); }
 
+// Blocks of a grid-stride kernel that are resident at once (at most
+// per_sm_cap per SM): its work is dealt out statically by block index, so a
+// block that has to wait for a second wave would finish last.
+template <class K>
+int resident_grid(int sm_count, K kernel, int per_sm_cap) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  return std::max(1, sm_count * std::min(per_sm, per_sm_cap));
+}
+
 // Builds the level-loop CUDA graph of a workspace.
 int build_exec(Workspace* ws) {
   GraphDev*   g = ws->g;
@@ -1244,7 +1255,7 @@ int build_exec(Workspace* ws) {
 
   cudaKernelNodeParams kp = {};
   kp.func                 = (void*)k_init;
-  kp.gridDim              = dim3(grid_for(g, 8));
+  kp.gridDim              = dim3(resident_grid(g->sm_count, k_init, 8));
   kp.blockDim             = dim3(kThreads);
   kp.kernelParams         = init_args;
   cudaGraphNode_t init_node;
@@ -1282,7 +1293,8 @@ int build_exec(Workspace* ws) {
   NWG_CUDA_TRY(cudaGraphAddNode(&switch_node, body, &decide_node, 1, &sp));
 
   void*     kernels[kNumActions] = {(void*)k_td, (void*)k_bu, (void*)k_b2q, (void*)k_td_loop};
-  const int grids[kNumActions]   = {grid_for(g, kTdPerSm), grid_for(g, 8), grid_for(g, 8), kSmallBlocks};
+  const int grids[kNumActions]   = {grid_for(g, kTdPerSm), resident_grid(g->sm_count, k_bu, 8),
+                                    resident_grid(g->sm_count, k_b2q, 8), kSmallBlocks};
   for (int a = 0; a < kNumActions; ++a) {
     void*                args[] = {&P};
     cudaKernelNodeParams ap     = {};
@@ -1412,9 +1424,11 @@ int run_stepped(const DobfsParams& params, int sm_count, uint32_t root, int alph
                 cudaStream_t stream) {
   DobfsParams P = params;
   P.set_cond    = 0;
-  const int big = std::max(1, sm_count * 8);
-  const int td  = std::max(1, sm_count * kTdPerSm);
-  k_init<<<big, kThreads, 0, stream>>>(P, root, (uint32_t)alpha, (uint32_t)beta, parents, 0u);
+  const int g_init = resident_grid(sm_count, k_init, 8);
+  const int g_bu   = resident_grid(sm_count, k_bu, 8);
+  const int g_b2q  = resident_grid(sm_count, k_b2q, 8);
+  const int td     = std::max(1, sm_count * kTdPerSm);
+  k_init<<<g_init, kThreads, 0, stream>>>(P, root, (uint32_t)alpha, (uint32_t)beta, parents, 0u);
   NWG_CUDA_TRY(cudaGetLastError());
   const uint64_t cap = 2 * P.n + 64;
   for (uint64_t step = 0; step <= cap; ++step) {
@@ -1429,9 +1443,9 @@ int run_stepped(const DobfsParams& params, int sm_count, uint32_t root, int alph
       void* args[] = {&P};
       NWG_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_td_loop, dim3(kSmallBlocks), dim3(kThreads), args, 0, stream));
     } else if (action == kActBU) {
-      k_bu<<<big, kThreads, 0, stream>>>(P);
+      k_bu<<<g_bu, kThreads, 0, stream>>>(P);
     } else if (action == kActB2Q) {
-      k_b2q<<<big, kThreads, 0, stream>>>(P);
+      k_b2q<<<g_b2q, kThreads, 0, stream>>>(P);
     } else {
       break;
     }

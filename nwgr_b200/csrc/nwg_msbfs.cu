@@ -424,9 +424,14 @@ __global__ void k_ms_decide(MsPassDev* d, cudaGraphConditionalHandle h_loop, cud
 // Grids of the grid-stride kernels: 8 blocks per SM, fewer when the largest
 // graph the workspace takes has less work than that, so the small graphs of
 // a serving mix leave room for other streams' launches.
-int grid_ms(const MsWorkspace* ws, uint64_t items, uint64_t per_block) {
+// ... and no more blocks than are resident at once: the kernels deal their
+// work out statically by block index, so a second wave would finish last.
+int grid_ms(const MsWorkspace* ws, const void* kernel, uint64_t items, uint64_t per_block) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kMsThreads, 0) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
   const uint64_t want = (items + per_block - 1) / per_block;
-  return (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)ws->sm_count * 8, want));
+  return (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)ws->sm_count * std::min(per_sm, 8), want));
 }
 
 // Node slots of a pass graph.
@@ -503,8 +508,13 @@ cudaKernelNodeParams ms_node_params(MsWorkspace* ws, MsArgs<W>& a, int slot, voi
   kp.blockDim             = dim3(kMsThreads);
   if (slot == kNRoots) kp.gridDim = dim3(1);
   else if (slot == kNList) kp.gridDim = dim3(1);
-  else if (slot == kNPush0 || slot == kNPush1) kp.gridDim = dim3(grid_ms(ws, ws->list_cap, kMsWarps));
-  else kp.gridDim = dim3(grid_ms(ws, ws->n_cap, kMsThreads));
+  else {
+    int& cached = ws->node_grid[W - 1][slot];  // occupancy queried once per workspace
+    if (!cached)
+      cached = (slot == kNPush0 || slot == kNPush1) ? grid_ms(ws, kp.func, ws->list_cap, kMsWarps)
+                                                    : grid_ms(ws, kp.func, ws->n_cap, kMsThreads);
+    kp.gridDim = dim3(cached);
+  }
   return kp;
 }
 
@@ -613,8 +623,9 @@ int ms_run_stepped(MsWorkspace* ws, MsArgs<W>& a, cudaStream_t stream) {
   MsPassDev* hd = static_cast<MsPassDev*>(ws->pass_host);
   k_ms_roots<W><<<1, kMsThreads, 0, stream>>>(a.base);
   k_ms_root_list<W><<<1, kMsThreads, 0, stream>>>(a.base);
-  const int g_list = grid_ms(ws, ws->list_cap, kMsWarps);
-  const int g_vert = grid_ms(ws, ws->n_cap, kMsThreads);
+  const int g_list = grid_ms(ws, (const void*)k_ms_push<W>, ws->list_cap, kMsWarps);
+  const int g_fin  = grid_ms(ws, (const void*)k_ms_finalize<W>, ws->n_cap, kMsThreads);
+  const int g_pull = grid_ms(ws, (const void*)k_ms_pull<W>, ws->n_cap, kMsThreads);
   for (;;) {
     k_ms_decide<<<1, 32, 0, stream>>>(d, cudaGraphConditionalHandle{}, cudaGraphConditionalHandle{}, 0);
     NWG_CUDA_TRY(cudaGetLastError());
@@ -624,10 +635,10 @@ int ms_run_stepped(MsWorkspace* ws, MsArgs<W>& a, cudaStream_t stream) {
     if (hd->stopped) break;
     MsParams<W>& q = a.par[hd->level & 1];
     if (hd->pull) {
-      k_ms_pull<W><<<g_vert, kMsThreads, 0, stream>>>(q);
+      k_ms_pull<W><<<g_pull, kMsThreads, 0, stream>>>(q);
     } else {
       k_ms_push<W><<<g_list, kMsThreads, 0, stream>>>(q);
-      k_ms_finalize<W><<<g_vert, kMsThreads, 0, stream>>>(q);
+      k_ms_finalize<W><<<g_fin, kMsThreads, 0, stream>>>(q);
     }
     NWG_CUDA_TRY(cudaGetLastError());
   }
