@@ -537,7 +537,7 @@ def main():
         e, v = g.component_edges(parents)
         e_r.append(e)
         n_r.append(v)
-        launches.append(2 * st.steps + 2)  # init + decide per iteration (+1 final) + one action per step
+        launches.append(st.kernel_launches)  # counted on the device
     e_r = np.asarray(e_r, np.float64)
     n_r = np.asarray(n_r, np.float64)
 

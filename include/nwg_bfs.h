@@ -69,6 +69,10 @@ typedef struct {
    * minus first_decide_ns), launch gaps included. */
   uint64_t trace_end_ns[NWG_TRACE_CAP];
   uint64_t first_decide_ns;
+  /* kernels the traversal launched (init, one decision per loop iteration,
+   * one action per iteration but the last; a persistent small-frontier
+   * action covers several steps in one launch) */
+  uint32_t kernel_launches;
 } nwg_bfs_stats;
 
 /* Library version string. */

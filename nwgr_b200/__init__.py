@@ -58,6 +58,7 @@ class Stats(C.Structure):
         ("trace_len", C.c_uint32), ("trace_dir", C.c_uint8 * TRACE_CAP),
         ("trace_frontier", C.c_uint64 * TRACE_CAP), ("trace_found", C.c_uint64 * TRACE_CAP),
         ("trace_end_ns", C.c_uint64 * TRACE_CAP), ("first_decide_ns", C.c_uint64),
+        ("kernel_launches", C.c_uint32),
     ]
 
     def trace(self):

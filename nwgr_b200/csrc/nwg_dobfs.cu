@@ -559,6 +559,7 @@ __device__ __forceinline__ void init_step(const DobfsParams& p, uint32_t root, u
     c.pre_decided = 0;
     p.ctrl->bar.count = 0;
     p.ctrl->err       = 0;
+    p.ctrl->decides   = 0;
     c.reached     = 1;
     c.t_start     = globaltimer();
     c.trace_len = 0;
@@ -705,6 +706,7 @@ __device__ uint32_t decide_core(const DobfsParams& p) {
 // decision to the graph's conditional handles.
 __global__ void k_decide(DobfsParams p) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  p.ctrl->decides++;  // only this thread writes it
   uint32_t next;
   if (__ldcg(&p.ctrl->h.pre_decided)) {
     next                  = __ldcg(&p.ctrl->h.action);
@@ -1474,6 +1476,8 @@ int zero_indegree_into(const uint64_t* in_off, uint64_t n, uint32_t* Z, int sm_c
 
 void fill_stats(const Ctrl& c, nwg_bfs_stats* s) {
   s->status    = c.h.status ? c.h.status : c.err;
+  // the init kernel, every decide, and one action after each decide but the last
+  s->kernel_launches = 2 * c.decides;
   s->steps     = c.h.steps;
   s->levels    = c.h.levels;
   s->td_steps  = c.h.td_steps;

@@ -88,6 +88,7 @@ struct Ctrl {
   CtrlHdr            h;
   GridBar            bar;
   int32_t            err;  // set with atomics by a device wait that ran out (never overwritten by the header copy)
+  uint32_t           decides;  // k_decide launches of the traversal (each loop iteration launches one)
   uint8_t            trace_dir[NWG_TRACE_CAP];
   unsigned long long trace_frontier[NWG_TRACE_CAP];
   unsigned long long trace_found[NWG_TRACE_CAP];
