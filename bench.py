@@ -30,6 +30,20 @@ cpu_baseline / --impl reference: the reference's own nw::graph::bfs
 (include/nwgraph/algorithms/bfs.hpp, compiled unmodified against the
 project's TBB-compatible thread pool, oracle/_ref) on this host's cores,
 timed like bench/common.hpp's time_op, on a bounded sample of the roots.
+
+Further sections of the same JSON line (each skippable with --no-<name>):
+  verifier     device BFSVerifier time per root, and the reference's
+               verifier on the host for the first root
+  batched      multi-source BFS on RMAT-22 with 64/256/1024 roots against 64
+               back-to-back single-source traversals
+  ragged       1000 small graphs x 4 roots in one persistent launch against
+               one call per item
+  serving      200 resident graphs, Poisson query rates 1k-200k/s, Zipf(1.1)
+               popularity: queries/s and p50/p99 latency
+  betweenness  brandes_bc over 64 sources on RMAT-22, beside the reference's
+               on a 4-source sample
+Profiling modes (one run inside the NVTX range nwg_profile, for ncu):
+--profile-one (single-source, host-stepped), --profile-msbfs, --profile-bc.
 """
 from __future__ import annotations
 
