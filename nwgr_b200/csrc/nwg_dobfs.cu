@@ -3,7 +3,7 @@
 // Restates nw::graph::bfs(out, in, root, num_bins, alpha, beta)
 // (include/nwgraph/algorithms/bfs.hpp:160-311 in NWGraph) as a CUDA graph:
 //
-//   k_init ──► WHILE(h_loop) { k_decide ──► SWITCH(h_switch) { k_td | k_bu | k_b2q | k_td(small grid) } }
+//   k_init ──► WHILE(h_loop) { k_decide ──► SWITCH(h_switch) { k_td | k_bu | k_b2q | k_td_loop | k_td_cluster } }
 //
 // k_decide is a one-thread kernel that reproduces the reference's integer
 // switch rules exactly (scout_count > edges_to_check / alpha selects
@@ -36,6 +36,7 @@
 // also carries such stale bits (curr is not cleared after bitmap->queue,
 // bfs.hpp:235-239).  Later pulls of the phase use the previous pull's C.
 #include <algorithm>
+#include <cooperative_groups.h>
 
 #include "nwg_internal.cuh"
 
@@ -49,6 +50,8 @@ constexpr int kBuLane      = 32;  // in-edges a lane scans alone before the warp
 constexpr int kTileWords   = 32;  // bitmap words per warp tile of the bitmap->queue pass (1024 vertices)
 constexpr int kBuTileWords = 8;   // bitmap words per pull tile (256 vertices)
 constexpr int kSmallBlocks = 64;  // grid of the small-frontier top-down branch
+constexpr int kClusterCtas = 8;   // the tiny-frontier branch: one cluster of this many blocks
+constexpr int kClusterUnits = kClusterCtas * (kThreads / 32);  // its work-unit limit: one per warp
 constexpr int kVisit       = 4;   // edges a lane claims per batch
 constexpr int kTdPerSm     = 3;   // k_td blocks per SM (80 registers per thread: 3 x 256 threads fill an SM)
 
@@ -614,7 +617,8 @@ __device__ uint32_t decide_core(const DobfsParams& p) {
       p.ctrl->t_first_decide = now - c.t_start;
       break;
     case kActTD:
-    case kActTDSmall: {
+    case kActTDSmall:
+    case kActTDCluster: {
       const uint32_t nxt = c.cur ^ 1u;
       const uint64_t nq  = frontier_size(c, nxt);
       trace_add(p.ctrl, c, 0, frontier_size(c, c.cur), nq, now);
@@ -682,7 +686,9 @@ __device__ uint32_t decide_core(const DobfsParams& p) {
       c.acc_scout = 0;
       // warp work units of the step: chunk entries + groups of 32 small vertices
       const uint64_t units = (c.qpos[c.cur] >> 32) + ((c.qpos[c.cur] & 0xFFFFFFFFull) + 31) / 32;
-      next                 = units <= (uint64_t)kSmallBlocks * kWarps ? kActTDSmall : kActTD;
+      next                 = units <= (uint64_t)kClusterUnits            ? kActTDCluster
+                             : units <= (uint64_t)kSmallBlocks * kWarps ? kActTDSmall
+                                                                        : kActTD;
     }
   }
   if (!done && ++c.steps > c.max_steps) {
@@ -887,6 +893,42 @@ __global__ void __launch_bounds__(kThreads) k_td_loop(DobfsParams p) {
     p.ctrl->h.pre_decided = 1;
   }
 }
+
+// k_td_cluster: consecutive tiny top-down levels in ONE thread-block cluster
+// (kClusterCtas blocks).  The level barriers are the cluster's hardware
+// barrier (barrier.cluster arrive/wait: release/acquire at cluster scope, so
+// the appends, counters and hub records of every block are visible after
+// it) instead of the global-memory grid barrier of k_td_loop, and no block
+// polls.  Rank 0 decides; every block reads that one decision from rank 0's
+// shared memory (distributed shared memory) after the second barrier, so all
+// blocks take the same branch and reach the same barriers.  Queue entries,
+// counters and hub records are read with L2 loads, as in k_td_loop.
+__global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kThreads) k_td_cluster(DobfsParams p) {
+  __shared__ TdWarp   s_tw[kWarps];
+  __shared__ uint32_t s_next;
+  namespace cg              = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  const uint32_t    rank    = cluster.block_rank();
+  const uint32_t    nblk    = cluster.num_blocks();
+  uint32_t* const   rank0_next = cluster.map_shared_rank(&s_next, 0);  // rank 0's copy, read over DSMEM
+  for (;;) {
+    const uint32_t wrote = td_step<true>(p, s_tw, rank, nblk);
+    cluster.sync();
+    expand_hubs(p, wrote, rank, nblk);
+    if (rank == 0 && threadIdx.x == 0) s_next = decide_core(p);
+    cluster.sync();
+    // every block reads the one decision rank 0 made; rank 0 writes it again
+    // only after the next level's first barrier, which all reads precede
+    const uint32_t next = *rank0_next;
+    if (next != kActTDCluster) break;
+  }
+  cluster.sync();  // rank 0's shared memory stays alive until every block has read it
+  if (rank == 0 && threadIdx.x == 0) {
+    __threadfence();
+    p.ctrl->h.pre_decided = 1;
+  }
+}
+
 
 // ---------------------------------------------------------------------------
 // Candidate compaction shared by k_bu and k_b2q: lane `lane` holds bitmap
@@ -1294,9 +1336,9 @@ int build_exec(Workspace* ws) {
   cudaGraphNode_t switch_node;
   NWG_CUDA_TRY(cudaGraphAddNode(&switch_node, body, &decide_node, 1, &sp));
 
-  void*     kernels[kNumActions] = {(void*)k_td, (void*)k_bu, (void*)k_b2q, (void*)k_td_loop};
+  void*     kernels[kNumActions] = {(void*)k_td, (void*)k_bu, (void*)k_b2q, (void*)k_td_loop, (void*)k_td_cluster};
   const int grids[kNumActions]   = {grid_for(g, kTdPerSm), resident_grid(g->sm_count, k_bu, 8),
-                                    resident_grid(g->sm_count, k_b2q, 8), kSmallBlocks};
+                                    resident_grid(g->sm_count, k_b2q, 8), kSmallBlocks, kClusterCtas};
   for (int a = 0; a < kNumActions; ++a) {
     void*                args[] = {&P};
     cudaKernelNodeParams ap     = {};
@@ -1444,6 +1486,8 @@ int run_stepped(const DobfsParams& params, int sm_count, uint32_t root, int alph
     } else if (action == kActTDSmall) {
       void* args[] = {&P};
       NWG_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_td_loop, dim3(kSmallBlocks), dim3(kThreads), args, 0, stream));
+    } else if (action == kActTDCluster) {
+      k_td_cluster<<<kClusterCtas, kThreads, 0, stream>>>(P);  // one cluster (compiled-in cluster size)
     } else if (action == kActBU) {
       k_bu<<<g_bu, kThreads, 0, stream>>>(P);
     } else if (action == kActB2Q) {

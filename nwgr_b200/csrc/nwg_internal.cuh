@@ -32,8 +32,9 @@ enum Action : uint32_t {
   kActBU      = 1,  // bottom-up pull
   kActB2Q     = 2,  // bitmap -> queue
   kActTDSmall = 3,  // top-down step on a small frontier, small grid
-  kActNone    = 4,
-  kNumActions = 4
+  kActTDCluster = 4,  // top-down step on a tiny frontier, one thread-block cluster
+  kActNone    = 5,
+  kNumActions = 5
 };
 
 struct Thresholds {
