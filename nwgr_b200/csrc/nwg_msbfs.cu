@@ -37,6 +37,7 @@ struct MsCounters {
   unsigned long long discovered;      // (source, vertex) pairs first reached this level
   unsigned long long frontier_edges;  // out-edges of the next frontier's vertices
   unsigned long long frontier_count;  // chunk entries in the next frontier list
+  unsigned long long alive[4];        // sources with a vertex in the next frontier (their BFS goes on)
 };
 
 constexpr uint32_t kMsChunk      = 256;  // out-edges per frontier chunk entry (one warp's push task)
@@ -84,6 +85,7 @@ struct MsParams {
   uint8_t*         depth;     // [k][n], rows of this pass start at depth + src0 * n
   uint64_t         full[W];   // mask of the valid sources of each word
   MsCounters*      cnt;       // counters of the level being produced
+  const MsCounters* prev;     // counters of the level before (its alive sources)
   const MsPassDev* d;
 };
 
@@ -134,7 +136,31 @@ __global__ void k_ms_roots(MsParams<W> p) {
   const uint64_t bit = 1ull << (s & 63);
   atomicOr((unsigned long long*)&p.vis[v * W + (s >> 6)], (unsigned long long)bit);
   atomicOr((unsigned long long*)&p.fr_nxt[v * W + (s >> 6)], (unsigned long long)bit);
+  atomicOr(&p.cnt->alive[s >> 6], (unsigned long long)bit);
   p.depth[(uint64_t)s * p.n + v] = 0;
+}
+
+// Sources seen in the new frontier, per warp in shared memory (lane 0 ORs
+// the warp's hardware OR-reduction of each word after every iteration), and
+// published with one atomic per word per block at the end of the kernel.
+template <int W>
+__device__ __forceinline__ void ms_seen_add(uint64_t (&slot)[4], const uint64_t (&nw)[W]) {
+#pragma unroll
+  for (int w = 0; w < W; ++w) {
+    const uint32_t lo = __reduce_or_sync(kFullMask, (uint32_t)nw[w]);
+    const uint32_t hi = __reduce_or_sync(kFullMask, (uint32_t)(nw[w] >> 32));
+    if ((threadIdx.x & 31) == 0 && (lo | hi)) slot[w] |= ((uint64_t)hi << 32) | lo;
+  }
+}
+
+template <int W>
+__device__ __forceinline__ void ms_seen_publish(const MsParams<W>& p, uint64_t (*seen)[4]) {
+  __syncthreads();
+  if (threadIdx.x < W) {
+    uint64_t x = 0;
+    for (int wp = 0; wp < kMsWarps; ++wp) x |= seen[wp][threadIdx.x];
+    if (x) atomicOr(&p.cnt->alive[threadIdx.x], (unsigned long long)x);
+  }
 }
 
 // Push: one warp per frontier chunk entry (up to kMsChunk out-edges of one
@@ -207,6 +233,9 @@ template <int W>
 __global__ void __launch_bounds__(kMsThreads) k_ms_finalize(MsParams<W> p) {
   const uint32_t level = p.d->level;
   unsigned long long disc = 0, fedges = 0;
+  __shared__ uint64_t s_seen[kMsWarps][4];
+  if ((threadIdx.x & 31) < 4) s_seen[threadIdx.x >> 5][threadIdx.x & 31] = 0;
+  __syncwarp();
   const uint64_t     stride = (uint64_t)gridDim.x * blockDim.x;
   const uint64_t     n_up   = (p.n + 31) & ~31ull;
   for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n_up; v += stride) {
@@ -230,8 +259,10 @@ __global__ void __launch_bounds__(kMsThreads) k_ms_finalize(MsParams<W> p) {
       }
     }
     write_depths<W>(p, level, has, v, nw);
+    ms_seen_add<W>(s_seen[threadIdx.x >> 5], nw);
     ms_append<W>(p, has, (uint32_t)v, fedges, has ? (unsigned long long)(p.off[v + 1] - p.off[v]) : 0ull);
   }
+  ms_seen_publish<W>(p, s_seen);
   const unsigned long long dsum = ms_block_sum(disc);
   const unsigned long long f    = ms_block_sum(fedges);
   if (threadIdx.x == 0) {
@@ -244,10 +275,15 @@ __global__ void __launch_bounds__(kMsThreads) k_ms_finalize(MsParams<W> p) {
 // in-neighbours' frontier words until every missing source is found.  Lists
 // longer than kMsLaneDeg are scanned by the whole warp afterwards.
 template <int W>
-__global__ void __launch_bounds__(kMsThreads) k_ms_pull(MsParams<W> p) {
+__global__ void __launch_bounds__(kMsThreads, W == 1 ? 5 : 3) k_ms_pull(MsParams<W> p) {
   const uint32_t level = p.d->level;
   const unsigned     lane   = threadIdx.x & 31;
   unsigned long long disc = 0, fedges = 0;
+  __shared__ uint64_t s_seen[kMsWarps][4];
+  __shared__ uint64_t s_act[4];  // sources that can still reach a vertex: valid, frontier not empty
+  if ((threadIdx.x & 31) < 4) s_seen[threadIdx.x >> 5][threadIdx.x & 31] = 0;
+  if (threadIdx.x < W) s_act[threadIdx.x] = p.full[threadIdx.x] & p.prev->alive[threadIdx.x];
+  __syncthreads();
   const uint64_t     stride = (uint64_t)gridDim.x * blockDim.x;
   const uint64_t     n_up   = (p.n + 31) & ~31ull;
   for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n_up; v += stride) {
@@ -255,11 +291,14 @@ __global__ void __launch_bounds__(kMsThreads) k_ms_pull(MsParams<W> p) {
     uint64_t   vis[W], acc[W];
     bool       need = false;
     const bool noin = !valid || ((__ldg(p.Z + (v >> 5)) >> (v & 31)) & 1u);
+    // only sources whose frontier is not empty can still reach v (s_act): a
+    // source in a small component must not keep every vertex scanning all
+    // its in-edges at every level
 #pragma unroll
     for (int w = 0; w < W; ++w) {
       vis[w] = valid ? p.vis[v * W + w] : p.full[w];
       acc[w] = 0;
-      need |= !noin && (vis[w] & p.full[w]) != p.full[w];
+      need |= !noin && (vis[w] & s_act[w]) != s_act[w];
     }
     uint64_t beg = 0, end = 0;
     if (need) {
@@ -282,7 +321,7 @@ __global__ void __launch_bounds__(kMsThreads) k_ms_pull(MsParams<W> p) {
       e   = min(lim, e + kMsProbe);
       sat = true;
 #pragma unroll
-      for (int w = 0; w < W; ++w) sat &= ((acc[w] | vis[w]) & p.full[w]) == p.full[w];
+      for (int w = 0; w < W; ++w) sat &= ((acc[w] | vis[w]) & s_act[w]) == s_act[w];
     }
     // long in-edge lists: the warp scans them together, 32 * kMsProbe in-edges per round
     unsigned pend = __ballot_sync(kFullMask, !sat && e < end);
@@ -322,7 +361,7 @@ __global__ void __launch_bounds__(kMsThreads) k_ms_pull(MsParams<W> p) {
 #pragma unroll
           for (int o = 16; o > 0; o >>= 1) x |= __shfl_xor_sync(kFullMask, x, o);
           a[w] = x;
-          done &= ((x | vs[w]) & p.full[w]) == p.full[w];
+          done &= ((x | vs[w]) & s_act[w]) == s_act[w];
         }
         if (done) break;
       }
@@ -344,8 +383,10 @@ __global__ void __launch_bounds__(kMsThreads) k_ms_pull(MsParams<W> p) {
       disc += __popcll(nw[w]);
     }
     write_depths<W>(p, level, has, v, nw);
+    ms_seen_add<W>(s_seen[threadIdx.x >> 5], nw);
     ms_append<W>(p, has, (uint32_t)v, fedges, has ? (unsigned long long)(p.off[v + 1] - p.off[v]) : 0ull);
   }
+  ms_seen_publish<W>(p, s_seen);
   const unsigned long long dsum = ms_block_sum(disc);
   const unsigned long long f    = ms_block_sum(fedges);
   if (threadIdx.x == 0) {
@@ -402,7 +443,7 @@ __global__ void k_ms_decide(MsPassDev* d, cudaGraphConditionalHandle h_loop, cud
     } else {
       const uint64_t fedges = prev.frontier_edges;
       d->nlist              = min((uint64_t)prev.frontier_count, d->list_cap);
-      d->cnt[L & 1]         = MsCounters{0, 0, 0};
+      d->cnt[L & 1]         = MsCounters{};
       const bool pull       = fedges > d->unchecked / (uint64_t)d->alpha;
       if (!pull) d->unchecked -= min(d->unchecked, fedges);
       if (L - 1 < kMsTrace) {
@@ -473,10 +514,12 @@ MsArgs<W> ms_args(GraphDev* g, MsWorkspace* ws, uint8_t* depth_rows, uint32_t k)
     q.list_cur     = ws->list[par ^ 1];
     q.list_nxt     = ws->list[par];
     q.cnt          = &d->cnt[par];
+    q.prev         = &d->cnt[par ^ 1];
   }
   p.fr_nxt   = ws->fr[0];
   p.list_nxt = ws->list[0];
   p.cnt      = &d->cnt[0];
+  p.prev     = &d->cnt[1];  // unused at level 0
   return a;
 }
 
