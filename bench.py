@@ -90,8 +90,9 @@ def parse():
     ap.add_argument("--no-verify", action="store_true")
     ap.add_argument("--no-bc", action="store_true")
     ap.add_argument("--profile-msbfs", action="store_true",
-                    help="one 64-source multi-source pass on RMAT-22, levels driven from the host, in NVTX range "
-                         "nwg_profile (for ncu)")
+                    help="one multi-source pass on RMAT-22 (--ms-sources roots), levels driven from the host, in "
+                         "NVTX range nwg_profile (for ncu)")
+    ap.add_argument("--ms-sources", type=int, default=64, help="sources of the --profile-msbfs pass (at most 256)")
     ap.add_argument("--profile-bc", action="store_true",
                     help="betweenness from one source on RMAT-22 in NVTX range nwg_profile (for ncu)")
     ap.add_argument("--serve-slots", type=int, default=16)
@@ -367,10 +368,11 @@ def profile_extension(args, torch):
     import nwgr_b200 as nwg
 
     g = nwg.Graph.rmat(22, 16, seed=GRAPH_SEED)
-    roots = g.roots(64, seed=ROOT_SEED)
+    roots = g.roots(max(64, args.ms_sources), seed=ROOT_SEED)
     if args.profile_msbfs:
+        roots = roots[: args.ms_sources]
         ws = nwg.MsWorkspace(g)
-        depths = torch.empty((64, g.n), dtype=torch.uint8, device="cuda")
+        depths = torch.empty((roots.size, g.n), dtype=torch.uint8, device="cuda")
         ws.run(roots, depths)
         torch.cuda.synchronize()
         torch.cuda.nvtx.range_push("nwg_profile")

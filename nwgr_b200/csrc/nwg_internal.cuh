@@ -165,14 +165,15 @@ struct MsWorkspace {
   uint64_t*       vis     = nullptr;
   uint64_t*       fr[2]   = {nullptr, nullptr};
   uint64_t*       nx      = nullptr;
+  uint64_t*       dp      = nullptr;  // 8 level bit-planes (depth bit j of each source), zero between passes
   uint64_t*       list[2] = {nullptr, nullptr};  // frontier chunk entries
   uint64_t        list_cap = 0;
   void*           pass_dev  = nullptr;  // arguments and level-loop state of a pass (device)
   void*           pass_host = nullptr;  // pinned staging of the same record
   cudaGraphExec_t exec[4] = {nullptr, nullptr, nullptr, nullptr};  // pass graphs, one per word count W
   cudaGraph_t     tmpl[4] = {nullptr, nullptr, nullptr, nullptr};  // their templates (own the nodes below)
-  cudaGraphNode_t nodes[4][8] = {};                                // kernel nodes updated per pass
-  int             node_grid[4][8] = {};                            // their grid sizes (resident blocks)
+  cudaGraphNode_t nodes[4][9] = {};                                // kernel nodes updated per pass
+  int             node_grid[4][9] = {};                            // their grid sizes (resident blocks)
   bool            stepped = false;      // host-driven levels (NWG_MS_STEPPED=1), for profilers
   cudaStream_t    stream  = nullptr;
   cudaEvent_t     ev0 = nullptr, ev1 = nullptr;

@@ -7,7 +7,10 @@
 //   VIS[n][W]    sources that have reached the vertex
 //   FR[2][n][W]  sources whose BFS has the vertex in its current / next frontier
 //   NX[n][W]     top-down accumulator (atomicOr), cleared when consumed
-//   depth[k][n]  uint8 output, 255 = unreached
+//   DP[8][n][W]  level bit-planes: bit s of DP[j][v][w] is bit j of the depth
+//                of v from source 64w + s; all zero between passes
+//   depth[k][n]  uint8 output, 255 = unreached, written once after the last
+//                level from VIS and DP (rows of 128 contiguous bytes per store)
 // Each level is either
 //   push: the vertices in the frontier list OR their frontier words into
 //         NX of their out-neighbours (64-bit atomicOr, only the bits the
@@ -43,6 +46,7 @@ struct MsCounters {
 constexpr uint32_t kMsChunk      = 256;  // out-edges per frontier chunk entry (one warp's push task)
 constexpr uint32_t kMsChunkShift = 8;
 constexpr uint64_t kMsLaneChunks = 16;  // a lane writes up to this many chunk entries of one vertex itself
+constexpr uint64_t kMsPlanes     = 8;   // level bit-planes: depths up to 254 (255 = unreached)
 
 // Level-loop state of a pass in device memory: the decide kernel advances
 // it, the level kernels read the level number and list length from it.
@@ -79,6 +83,8 @@ struct MsParams {
   uint64_t*        fr_cur;
   uint64_t*        fr_nxt;
   uint64_t*        nx;
+  uint64_t*        dp;        // level bit-planes, plane j at dp + j * plane
+  uint64_t         plane;     // words per plane (n * W)
   uint64_t*        list_cur;  // frontier chunk entries (vertex << 32 | chunk), push input
   uint64_t*        list_nxt;
   uint64_t         list_cap;
@@ -107,27 +113,111 @@ __device__ __forceinline__ T ms_block_sum(T v) {
   return t;  // valid in thread 0
 }
 
-// depth[s][v] = level for every source bit s newly set at v.  Lanes hold
-// consecutive vertices; the warp walks only the bits some lane has, so each
-// store instruction writes one row's bytes for up to 32 adjacent vertices.
+// The sources in nw first reach v at `level`: OR them into the planes of
+// the level's set bits (at most three words for levels below 16).  Only
+// v's own thread touches v's plane words in a level, and kernel boundaries
+// order the levels, so a plain read-modify-write is enough.  A warp's lanes
+// hold consecutive vertices, so each plane access is one coalesced run.
 template <int W>
-__device__ __forceinline__ void write_depths(const MsParams<W>& p, uint32_t level, bool has, uint64_t v,
+__device__ __forceinline__ void record_level(const MsParams<W>& p, uint32_t level, uint64_t v,
                                              const uint64_t (&nw)[W]) {
 #pragma unroll
   for (int w = 0; w < W; ++w) {
-    uint64_t any = has ? nw[w] : 0ull;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) any |= __shfl_xor_sync(kFullMask, any, o);
-    while (any) {
-      const int s = __ffsll((long long)any) - 1;
-      any &= any - 1;
-      if (has && ((nw[w] >> s) & 1ull)) p.depth[(uint64_t)(w * 64 + s) * p.n + v] = (uint8_t)level;
+    if (!nw[w]) continue;
+    for (uint32_t b = level; b; b &= b - 1) {
+      uint64_t* q = p.dp + (uint64_t)(__ffs(b) - 1) * p.plane + v * W + w;
+      *q |= nw[w];
     }
   }
 }
 
-// Roots: VIS, FR[cur] and depth 0 for each source; the frontier list holds
-// the distinct roots (deduplicated on the host).
+// spread4(x), x < 16: bit t of x to bit 0 of byte t.  The four partial
+// products x, x << 7, x << 14, x << 21 occupy disjoint bit ranges, so the
+// multiply never carries.
+__device__ __forceinline__ uint32_t spread4(uint32_t x) { return (x * 0x00204081u) & 0x01010101u; }
+
+// Depth rows of one warp tile: 128 consecutive vertices (4 per lane) of one
+// source word, P planes.  Per group of 4 sources a lane forms, for each of
+// its vertices, the 4 depth bytes (255 where VIS lacks the bit), then
+// transposes the 4x4 bytes with byte permutes so that each 32-bit store
+// writes one source row's bytes for the lane's 4 vertices: 128 contiguous
+// bytes of a row per warp store.  The planes read are cleared.
+template <int W, int P>
+__device__ __forceinline__ void depth_tile(const MsParams<W>& p, int planes, uint64_t v0, int w, int nsrc,
+                                           bool aligned) {
+  const uint64_t n = p.n;
+  uint64_t       vis[4], pl[4][P];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const uint64_t v  = v0 + i;
+    const bool     ok = v < n;
+    vis[i]            = ok ? p.vis[v * W + w] : 0ull;
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+      pl[i][j] = 0;
+      if (ok && j < planes) {
+        uint64_t* q = p.dp + (uint64_t)j * p.plane + v * W + w;
+        pl[i][j]    = *q;
+        if (pl[i][j]) *q = 0;
+      }
+    }
+  }
+#pragma unroll
+  for (int s0 = 0; s0 < 64; s0 += 4) {
+    if (s0 >= nsrc) break;
+    uint32_t b[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      uint32_t d = 0;
+#pragma unroll
+      for (int j = 0; j < P; ++j) d |= spread4((uint32_t)(pl[i][j] >> s0) & 15u) << j;
+      const uint32_t m = spread4((uint32_t)(vis[i] >> s0) & 15u) * 0xFFu;
+      b[i]             = d | ~m;
+    }
+    const uint32_t x01l = __byte_perm(b[0], b[1], 0x5140), x01h = __byte_perm(b[0], b[1], 0x7362);
+    const uint32_t x23l = __byte_perm(b[2], b[3], 0x5140), x23h = __byte_perm(b[2], b[3], 0x7362);
+    const uint32_t row[4] = {__byte_perm(x01l, x23l, 0x5410), __byte_perm(x01l, x23l, 0x7632),
+                             __byte_perm(x01h, x23h, 0x5410), __byte_perm(x01h, x23h, 0x7632)};
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      if (s0 + t >= nsrc) break;
+      uint8_t* dst = p.depth + (uint64_t)(64 * w + s0 + t) * n + v0;
+      if (aligned && v0 + 3 < n) {
+        *reinterpret_cast<uint32_t*>(dst) = row[t];
+      } else {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          if (v0 + i < n) dst[i] = (uint8_t)(row[t] >> (8 * i));
+      }
+    }
+  }
+}
+
+// After the last level: every depth row of the pass from VIS and the level
+// planes (the planes in use are those of the highest level run), and those
+// planes cleared for the next pass.  Replaces a 255-fill of the rows and
+// the per-level byte stores of each discovery.
+template <int W>
+__global__ void __launch_bounds__(kMsThreads) k_ms_depths(MsParams<W> p) {
+  const uint32_t top    = p.d->level;
+  const int      planes = top ? 32 - __clz(top) : 0;
+  const int      k      = (int)p.d->k;
+  const unsigned lane   = threadIdx.x & 31;
+  const uint64_t tiles  = (p.n + 127) / 128 * W;
+  const uint64_t gwarp  = (uint64_t)blockIdx.x * kMsWarps + (threadIdx.x >> 5);
+  const uint64_t nwarps = (uint64_t)gridDim.x * kMsWarps;
+  const bool     aligned = ((reinterpret_cast<uintptr_t>(p.depth) | p.n) & 3u) == 0;
+  for (uint64_t t = gwarp; t < tiles; t += nwarps) {
+    const int      w    = (int)(t % W);  // words of the same vertices in adjacent warps: shared VIS sectors
+    const uint64_t v0   = (t / W) * 128 + lane * 4;
+    const int      nsrc = min(64, k - 64 * w);
+    if (planes <= 4) depth_tile<W, 4>(p, planes, v0, w, nsrc, aligned);
+    else depth_tile<W, 8>(p, planes, v0, w, nsrc, aligned);
+  }
+}
+
+// Roots: VIS and FR[cur] for each source (depth 0: no plane bits); the
+// frontier list holds the distinct roots (deduplicated on the host).
 template <int W>
 __global__ void k_ms_roots(MsParams<W> p) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -137,7 +227,6 @@ __global__ void k_ms_roots(MsParams<W> p) {
   atomicOr((unsigned long long*)&p.vis[v * W + (s >> 6)], (unsigned long long)bit);
   atomicOr((unsigned long long*)&p.fr_nxt[v * W + (s >> 6)], (unsigned long long)bit);
   atomicOr(&p.cnt->alive[s >> 6], (unsigned long long)bit);
-  p.depth[(uint64_t)s * p.n + v] = 0;
 }
 
 // Sources seen in the new frontier, per warp in shared memory (lane 0 ORs
@@ -258,7 +347,7 @@ __global__ void __launch_bounds__(kMsThreads) k_ms_finalize(MsParams<W> p) {
         disc += __popcll(nw[w]);
       }
     }
-    write_depths<W>(p, level, has, v, nw);
+    if (has) record_level<W>(p, level, v, nw);
     ms_seen_add<W>(s_seen[threadIdx.x >> 5], nw);
     ms_append<W>(p, has, (uint32_t)v, fedges, has ? (unsigned long long)(p.off[v + 1] - p.off[v]) : 0ull);
   }
@@ -382,7 +471,7 @@ __global__ void __launch_bounds__(kMsThreads, W == 1 ? 5 : 3) k_ms_pull(MsParams
       has |= nw[w] != 0;
       disc += __popcll(nw[w]);
     }
-    write_depths<W>(p, level, has, v, nw);
+    if (has) record_level<W>(p, level, v, nw);
     ms_seen_add<W>(s_seen[threadIdx.x >> 5], nw);
     ms_append<W>(p, has, (uint32_t)v, fedges, has ? (unsigned long long)(p.off[v + 1] - p.off[v]) : 0ull);
   }
@@ -476,7 +565,7 @@ int grid_ms(const MsWorkspace* ws, const void* kernel, uint64_t items, uint64_t 
 }
 
 // Node slots of a pass graph.
-enum { kNRoots, kNList, kNPush0, kNFin0, kNPull0, kNPush1, kNFin1, kNPull1, kNNodes };
+enum { kNRoots, kNList, kNPush0, kNFin0, kNPull0, kNPush1, kNFin1, kNPull1, kNDepths, kNNodes };
 
 // Arguments of a pass: the base set (roots, level 0) and the two parities.
 template <int W>
@@ -498,6 +587,8 @@ MsArgs<W> ms_args(GraphDev* g, MsWorkspace* ws, uint8_t* depth_rows, uint32_t k)
   p.n        = g->n;
   p.vis      = ws->vis;
   p.nx       = ws->nx;
+  p.dp       = ws->dp;
+  p.plane    = g->n * W;
   p.list_cap = ws->list_cap;
   p.depth    = depth_rows;
   for (int w = 0; w < W; ++w) {
@@ -532,13 +623,14 @@ void* ms_node_fn(int slot) {
     case kNPush1: return (void*)k_ms_push<W>;
     case kNFin0:
     case kNFin1: return (void*)k_ms_finalize<W>;
+    case kNDepths: return (void*)k_ms_depths<W>;
     default: return (void*)k_ms_pull<W>;
   }
 }
 
 template <int W>
 MsParams<W>* ms_node_args(MsArgs<W>& a, int slot) {
-  if (slot == kNRoots || slot == kNList) return &a.base;
+  if (slot == kNRoots || slot == kNList || slot == kNDepths) return &a.base;
   return slot < kNPush1 ? &a.par[1] : &a.par[0];  // the first half of the body runs odd levels
 }
 
@@ -555,7 +647,8 @@ cudaKernelNodeParams ms_node_params(MsWorkspace* ws, MsArgs<W>& a, int slot, voi
     int& cached = ws->node_grid[W - 1][slot];  // occupancy queried once per workspace
     if (!cached)
       cached = (slot == kNPush0 || slot == kNPush1) ? grid_ms(ws, kp.func, ws->list_cap, kMsWarps)
-                                                    : grid_ms(ws, kp.func, ws->n_cap, kMsThreads);
+               : slot == kNDepths ? grid_ms(ws, kp.func, (ws->n_cap + 127) / 128 * W, kMsWarps)
+                                  : grid_ms(ws, kp.func, ws->n_cap, kMsThreads);
     kp.gridDim = dim3(cached);
   }
   return kp;
@@ -563,7 +656,8 @@ cudaKernelNodeParams ms_node_params(MsWorkspace* ws, MsArgs<W>& a, int slot, voi
 
 // The pass as a CUDA graph: roots, first frontier list, then
 // WHILE(decide -> SWITCH{push + finalize | pull} for an odd level, the same
-// for the following even level); no host round trip per level.
+// for the following even level), then the depth rows; no host round trip
+// per level.
 template <int W>
 int ms_build_exec(MsWorkspace* ws, MsArgs<W>& a) {
   MsPassDev*  d = static_cast<MsPassDev*>(ws->pass_dev);
@@ -620,6 +714,7 @@ int ms_build_exec(MsWorkspace* ws, MsArgs<W>& a) {
       return fail(e, "level nodes");
     prev = n_sw;
   }
+  if ((e = add(graph, &n_while, kNDepths)) != cudaSuccess) return fail(e, "depth rows node");
   cudaGraphExec_t exec;
   if ((e = cudaGraphInstantiate(&exec, graph, 0)) != cudaSuccess) return fail(e, "multi-source graph instantiate");
   if (ws->tmpl[W - 1]) cudaGraphDestroy(ws->tmpl[W - 1]);
@@ -685,12 +780,16 @@ int ms_run_stepped(MsWorkspace* ws, MsArgs<W>& a, cudaStream_t stream) {
     }
     NWG_CUDA_TRY(cudaGetLastError());
   }
+  k_ms_depths<W><<<grid_ms(ws, (const void*)k_ms_depths<W>, (ws->n_cap + 127) / 128 * W, kMsWarps), kMsThreads, 0,
+                   stream>>>(a.base);
+  NWG_CUDA_TRY(cudaGetLastError());
   return NWG_OK;
 }
 
 // One pass of up to 64 * W sources: the host writes the pass record (one
 // copy from pinned memory), clears the state, launches the pass graph and
-// reads the record back once at the end.
+// reads the record back once at the end.  Every byte of the k depth rows is
+// written by the pass's last kernel (no fill beforehand).
 template <int W>
 int ms_pass(GraphDev* g, MsWorkspace* ws, const uint32_t* roots_host, uint32_t k, uint8_t* depth_rows, int alpha,
             cudaStream_t stream, nwg_msbfs_stats* st) {
@@ -715,7 +814,6 @@ int ms_pass(GraphDev* g, MsWorkspace* ws, const uint32_t* roots_host, uint32_t k
   NWG_CUDA_TRY(cudaMemsetAsync(ws->vis, 0, words, stream));
   NWG_CUDA_TRY(cudaMemsetAsync(ws->fr[0], 0, words, stream));
   NWG_CUDA_TRY(cudaMemsetAsync(ws->nx, 0, words, stream));
-  NWG_CUDA_TRY(cudaMemsetAsync(depth_rows, 0xFF, (size_t)k * n, stream));
   NWG_CUDA_TRY(cudaMemcpyAsync(dd, &h, sizeof h, cudaMemcpyHostToDevice, stream));
   if (ws->stepped) {
     int rc = ms_run_stepped<W>(ws, a, stream);
@@ -749,9 +847,10 @@ int ms_pass(GraphDev* g, MsWorkspace* ws, const uint32_t* roots_host, uint32_t k
 
 uint64_t ms_ws_bytes(uint64_t n_cap, uint64_t m_cap) {
   const uint64_t n = std::max<uint64_t>(n_cap, 1);
-  // VIS, FR[2], NX at four words per vertex, two frontier lists (every
-  // frontier vertex has at most deg / kMsChunk + 1 entries), the pass record
-  return 4 * n * 4 * sizeof(uint64_t) + 2 * (n + m_cap / kMsChunk + 1) * 8 + sizeof(MsPassDev);
+  // VIS, FR[2], NX and the 8 level planes at four words per vertex, two
+  // frontier lists (every frontier vertex has at most deg / kMsChunk + 1
+  // entries), the pass record
+  return (4 + kMsPlanes) * n * 4 * sizeof(uint64_t) + 2 * (n + m_cap / kMsChunk + 1) * 8 + sizeof(MsPassDev);
 }
 
 int ms_ws_init_cap(GraphDev* g, uint64_t n_cap, uint64_t m_cap, MsWorkspace* ws) {
@@ -769,12 +868,14 @@ int ms_ws_init_cap(GraphDev* g, uint64_t n_cap, uint64_t m_cap, MsWorkspace* ws)
   NWG_CUDA_TRY(cudaDeviceGetAttribute(&ws->sm_count, cudaDevAttrMultiProcessorCount, dev));
   if (cudaMalloc(&ws->vis, words) != cudaSuccess || cudaMalloc(&ws->fr[0], words) != cudaSuccess ||
       cudaMalloc(&ws->fr[1], words) != cudaSuccess || cudaMalloc(&ws->nx, words) != cudaSuccess ||
+      cudaMalloc(&ws->dp, kMsPlanes * words) != cudaSuccess ||
       cudaMalloc(&ws->list[0], list_cap * 8) != cudaSuccess || cudaMalloc(&ws->list[1], list_cap * 8) != cudaSuccess ||
       cudaMalloc(&ws->pass_dev, sizeof(MsPassDev)) != cudaSuccess ||
       cudaMallocHost(&ws->pass_host, sizeof(MsPassDev)) != cudaSuccess) {
     cudaGetLastError();
     return set_error(NWG_ENOMEM, "multi-source workspace allocation failed");
   }
+  NWG_CUDA_TRY(cudaMemset(ws->dp, 0, kMsPlanes * words));  // the planes start (and end every pass) zero
   NWG_CUDA_TRY(cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking));
   NWG_CUDA_TRY(cudaEventCreate(&ws->ev0));
   NWG_CUDA_TRY(cudaEventCreate(&ws->ev1));
@@ -801,6 +902,7 @@ void ms_ws_free(MsWorkspace* ws) {
   cudaFree(ws->fr[0]);
   cudaFree(ws->fr[1]);
   cudaFree(ws->nx);
+  cudaFree(ws->dp);
   cudaFree(ws->list[0]);
   cudaFree(ws->list[1]);
   cudaFree(ws->pass_dev);
