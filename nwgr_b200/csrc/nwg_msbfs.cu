@@ -10,7 +10,7 @@
 //   DP[8][n][W]  level bit-planes: bit s of DP[j][v][w] is bit j of the depth
 //                of v from source 64w + s; all zero between passes
 //   depth[k][n]  uint8 output, 255 = unreached, written once after the last
-//                level from VIS and DP (rows of 128 contiguous bytes per store)
+//                level from VIS and DP (rows of 64 contiguous bytes per store)
 // Each level is either
 //   push: the vertices in the frontier list OR their frontier words into
 //         NX of their out-neighbours (64-bit atomicOr, only the bits the
@@ -136,19 +136,20 @@ __device__ __forceinline__ void record_level(const MsParams<W>& p, uint32_t leve
 // multiply never carries.
 __device__ __forceinline__ uint32_t spread4(uint32_t x) { return (x * 0x00204081u) & 0x01010101u; }
 
-// Depth rows of one warp tile: 128 consecutive vertices (4 per lane) of one
+// Depth rows of one warp tile: 64 consecutive vertices (2 per lane) of one
 // source word, P planes.  Per group of 4 sources a lane forms, for each of
-// its vertices, the 4 depth bytes (255 where VIS lacks the bit), then
-// transposes the 4x4 bytes with byte permutes so that each 32-bit store
-// writes one source row's bytes for the lane's 4 vertices: 128 contiguous
-// bytes of a row per warp store.  The planes read are cleared.
+// its vertices, the 4 depth bytes (255 where VIS lacks the bit), then pairs
+// them with byte permutes so that each 16-bit store writes one source row's
+// bytes for the lane's 2 vertices: 64 contiguous bytes of a row per warp
+// store.  Two vertices per lane keep the kernel near 64 registers, so four
+// blocks fit an SM and hide the load latency.  The planes read are cleared.
 template <int W, int P>
 __device__ __forceinline__ void depth_tile(const MsParams<W>& p, int planes, uint64_t v0, int w, int nsrc,
                                            bool aligned) {
   const uint64_t n = p.n;
-  uint64_t       vis[4], pl[4][P];
+  uint64_t       vis[2], pl[2][P];
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
+  for (int i = 0; i < 2; ++i) {
     const uint64_t v  = v0 + i;
     const bool     ok = v < n;
     vis[i]            = ok ? p.vis[v * W + w] : 0ull;
@@ -165,29 +166,25 @@ __device__ __forceinline__ void depth_tile(const MsParams<W>& p, int planes, uin
 #pragma unroll
   for (int s0 = 0; s0 < 64; s0 += 4) {
     if (s0 >= nsrc) break;
-    uint32_t b[4];
+    uint32_t b[2];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < 2; ++i) {
       uint32_t d = 0;
 #pragma unroll
       for (int j = 0; j < P; ++j) d |= spread4((uint32_t)(pl[i][j] >> s0) & 15u) << j;
       const uint32_t m = spread4((uint32_t)(vis[i] >> s0) & 15u) * 0xFFu;
       b[i]             = d | ~m;
     }
-    const uint32_t x01l = __byte_perm(b[0], b[1], 0x5140), x01h = __byte_perm(b[0], b[1], 0x7362);
-    const uint32_t x23l = __byte_perm(b[2], b[3], 0x5140), x23h = __byte_perm(b[2], b[3], 0x7362);
-    const uint32_t row[4] = {__byte_perm(x01l, x23l, 0x5410), __byte_perm(x01l, x23l, 0x7632),
-                             __byte_perm(x01h, x23h, 0x5410), __byte_perm(x01h, x23h, 0x7632)};
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
       if (s0 + t >= nsrc) break;
-      uint8_t* dst = p.depth + (uint64_t)(64 * w + s0 + t) * n + v0;
-      if (aligned && v0 + 3 < n) {
-        *reinterpret_cast<uint32_t*>(dst) = row[t];
+      const uint32_t row = __byte_perm(b[0], b[1], (uint32_t)(t | ((4 + t) << 4)));  // byte t of each vertex
+      uint8_t*       dst = p.depth + (uint64_t)(64 * w + s0 + t) * n + v0;
+      if (aligned && v0 + 1 < n) {
+        *reinterpret_cast<uint16_t*>(dst) = (uint16_t)row;
       } else {
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-          if (v0 + i < n) dst[i] = (uint8_t)(row[t] >> (8 * i));
+        dst[0] = (uint8_t)row;
+        if (v0 + 1 < n) dst[1] = (uint8_t)(row >> 8);
       }
     }
   }
@@ -198,20 +195,22 @@ __device__ __forceinline__ void depth_tile(const MsParams<W>& p, int planes, uin
 // planes cleared for the next pass.  Replaces a 255-fill of the rows and
 // the per-level byte stores of each discovery.
 template <int W>
-__global__ void __launch_bounds__(kMsThreads) k_ms_depths(MsParams<W> p) {
+__global__ void __launch_bounds__(kMsThreads, 4) k_ms_depths(MsParams<W> p) {
   const uint32_t top    = p.d->level;
   const int      planes = top ? 32 - __clz(top) : 0;
   const int      k      = (int)p.d->k;
   const unsigned lane   = threadIdx.x & 31;
-  const uint64_t tiles  = (p.n + 127) / 128 * W;
+  const uint64_t tiles  = (p.n + 63) / 64 * W;
   const uint64_t gwarp  = (uint64_t)blockIdx.x * kMsWarps + (threadIdx.x >> 5);
   const uint64_t nwarps = (uint64_t)gridDim.x * kMsWarps;
-  const bool     aligned = ((reinterpret_cast<uintptr_t>(p.depth) | p.n) & 3u) == 0;
+  const bool     aligned = ((reinterpret_cast<uintptr_t>(p.depth) | p.n) & 1u) == 0;
   for (uint64_t t = gwarp; t < tiles; t += nwarps) {
     const int      w    = (int)(t % W);  // words of the same vertices in adjacent warps: shared VIS sectors
-    const uint64_t v0   = (t / W) * 128 + lane * 4;
+    const uint64_t v0   = (t / W) * 64 + lane * 2;
     const int      nsrc = min(64, k - 64 * w);
-    if (planes <= 4) depth_tile<W, 4>(p, planes, v0, w, nsrc, aligned);
+    if (v0 >= p.n) continue;
+    if (planes <= 3) depth_tile<W, 3>(p, planes, v0, w, nsrc, aligned);
+    else if (planes <= 4) depth_tile<W, 4>(p, planes, v0, w, nsrc, aligned);
     else depth_tile<W, 8>(p, planes, v0, w, nsrc, aligned);
   }
 }
@@ -647,7 +646,7 @@ cudaKernelNodeParams ms_node_params(MsWorkspace* ws, MsArgs<W>& a, int slot, voi
     int& cached = ws->node_grid[W - 1][slot];  // occupancy queried once per workspace
     if (!cached)
       cached = (slot == kNPush0 || slot == kNPush1) ? grid_ms(ws, kp.func, ws->list_cap, kMsWarps)
-               : slot == kNDepths ? grid_ms(ws, kp.func, (ws->n_cap + 127) / 128 * W, kMsWarps)
+               : slot == kNDepths ? grid_ms(ws, kp.func, (ws->n_cap + 63) / 64 * W, kMsWarps)
                                   : grid_ms(ws, kp.func, ws->n_cap, kMsThreads);
     kp.gridDim = dim3(cached);
   }
@@ -780,7 +779,7 @@ int ms_run_stepped(MsWorkspace* ws, MsArgs<W>& a, cudaStream_t stream) {
     }
     NWG_CUDA_TRY(cudaGetLastError());
   }
-  k_ms_depths<W><<<grid_ms(ws, (const void*)k_ms_depths<W>, (ws->n_cap + 127) / 128 * W, kMsWarps), kMsThreads, 0,
+  k_ms_depths<W><<<grid_ms(ws, (const void*)k_ms_depths<W>, (ws->n_cap + 63) / 64 * W, kMsWarps), kMsThreads, 0,
                    stream>>>(a.base);
   NWG_CUDA_TRY(cudaGetLastError());
   return NWG_OK;
