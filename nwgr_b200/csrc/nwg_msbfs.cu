@@ -131,6 +131,25 @@ __device__ __forceinline__ void record_level(const MsParams<W>& p, uint32_t leve
   }
 }
 
+// The W words of one vertex (read-only during the kernel) with 16-byte
+// loads where W is even: a vertex's words start 16-byte aligned then (the
+// arrays are 256-byte aligned and each vertex owns W consecutive words), so
+// two words come per load instruction instead of one.
+template <int W>
+__device__ __forceinline__ void ms_words(const uint64_t* __restrict__ src, uint64_t (&x)[W]) {
+  if constexpr (W % 2 == 0) {
+#pragma unroll
+    for (int w = 0; w < W; w += 2) {
+      const ulonglong2 t = __ldg(reinterpret_cast<const ulonglong2*>(src + w));
+      x[w]               = t.x;
+      x[w + 1]           = t.y;
+    }
+  } else {
+#pragma unroll
+    for (int w = 0; w < W; ++w) x[w] = __ldg(src + w);
+  }
+}
+
 // spread4(x), x < 16: bit t of x to bit 0 of byte t.  The four partial
 // products x, x << 7, x << 14, x << 21 occupy disjoint bit ranges, so the
 // multiply never carries.
@@ -263,15 +282,16 @@ __global__ void __launch_bounds__(kMsThreads) k_ms_push(MsParams<W> p) {
     const uint64_t ent = p.list_cur[i];
     const uint32_t u   = (uint32_t)(ent >> 32);
     uint64_t       f[W];
-#pragma unroll
-    for (int w = 0; w < W; ++w) f[w] = p.fr_cur[(uint64_t)u * W + w];
+    ms_words<W>(p.fr_cur + (uint64_t)u * W, f);
     const uint64_t beg = p.off[u] + ((ent & 0xFFFFFFFFull) << kMsChunkShift);
     const uint64_t end = min(p.off[u + 1], beg + kMsChunk);
     for (uint64_t e = beg + lane; e < end; e += 32) {
       const uint32_t v = __ldg(p.col + e);
+      uint64_t       seen[W];
+      ms_words<W>(p.vis + (uint64_t)v * W, seen);  // VIS is stable during the push
 #pragma unroll
       for (int w = 0; w < W; ++w) {
-        const uint64_t m = f[w] & ~p.vis[(uint64_t)v * W + w];  // VIS is stable during the push
+        const uint64_t m = f[w] & ~seen[w];
         if (m) atomicOr((unsigned long long*)&p.nx[(uint64_t)v * W + w], (unsigned long long)m);
       }
     }
@@ -403,8 +423,10 @@ __global__ void __launch_bounds__(kMsThreads, W == 1 ? 5 : 3) k_ms_pull(MsParams
 #pragma unroll
       for (int q = 0; q < kMsProbe; ++q)
         if (u[q] != kNull) {
+          uint64_t x[W];
+          ms_words<W>(p.fr_cur + (uint64_t)u[q] * W, x);
 #pragma unroll
-          for (int w = 0; w < W; ++w) acc[w] |= p.fr_cur[(uint64_t)u[q] * W + w];
+          for (int w = 0; w < W; ++w) acc[w] |= x[w];
         }
       e   = min(lim, e + kMsProbe);
       sat = true;
@@ -439,8 +461,10 @@ __global__ void __launch_bounds__(kMsThreads, W == 1 ? 5 : 3) k_ms_pull(MsParams
 #pragma unroll
         for (int q = 0; q < kMsProbe; ++q)
           if (u[q] != kNull) {
+            uint64_t x[W];
+            ms_words<W>(p.fr_cur + (uint64_t)u[q] * W, x);
 #pragma unroll
-            for (int w = 0; w < W; ++w) mine[w] |= p.fr_cur[(uint64_t)u[q] * W + w];
+            for (int w = 0; w < W; ++w) mine[w] |= x[w];
           }
         bool done = true;
 #pragma unroll
