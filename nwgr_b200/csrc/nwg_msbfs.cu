@@ -383,7 +383,7 @@ __global__ void __launch_bounds__(kMsThreads) k_ms_finalize(MsParams<W> p) {
 // in-neighbours' frontier words until every missing source is found.  Lists
 // longer than kMsLaneDeg are scanned by the whole warp afterwards.
 template <int W>
-__global__ void __launch_bounds__(kMsThreads, W == 1 ? 5 : 3) k_ms_pull(MsParams<W> p) {
+__global__ void __launch_bounds__(kMsThreads, W == 1 ? 5 : 4) k_ms_pull(MsParams<W> p) {
   const uint32_t level = p.d->level;
   const unsigned     lane   = threadIdx.x & 31;
   unsigned long long disc = 0, fedges = 0;
