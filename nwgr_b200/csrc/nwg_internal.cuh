@@ -173,7 +173,7 @@ struct MsWorkspace {
   cudaGraphExec_t exec[4] = {nullptr, nullptr, nullptr, nullptr};  // pass graphs, one per word count W
   cudaGraph_t     tmpl[4] = {nullptr, nullptr, nullptr, nullptr};  // their templates (own the nodes below)
   cudaGraphNode_t nodes[4][9] = {};                                // kernel nodes updated per pass
-  int             node_grid[4][9] = {};                            // their grid sizes (resident blocks)
+  int             node_occ[4][9] = {};                             // their resident blocks per SM
   bool            stepped = false;      // host-driven levels (NWG_MS_STEPPED=1), for profilers
   cudaStream_t    stream  = nullptr;
   cudaEvent_t     ev0 = nullptr, ev1 = nullptr;

@@ -574,17 +574,25 @@ __global__ void k_ms_decide(MsPassDev* d, cudaGraphConditionalHandle h_loop, cud
   }
 }
 
-// Grids of the grid-stride kernels: 8 blocks per SM, fewer when the largest
-// graph the workspace takes has less work than that, so the small graphs of
-// a serving mix leave room for other streams' launches.
-// ... and no more blocks than are resident at once: the kernels deal their
-// work out statically by block index, so a second wave would finish last.
-int grid_ms(const MsWorkspace* ws, const void* kernel, uint64_t items, uint64_t per_block) {
+// Grids of the grid-stride kernels: at most 8 blocks per SM and no more
+// than are resident at once (the kernels deal their work out statically by
+// block index, so a second wave would finish last), fewer when the pass's
+// graph has less work than that, so the small graphs of a serving mix leave
+// room for other streams' launches.
+int ms_occupancy(const void* kernel) {
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kMsThreads, 0) != cudaSuccess || per_sm < 1)
     per_sm = 1;
+  return per_sm;
+}
+
+int grid_for(const MsWorkspace* ws, int per_sm, uint64_t items, uint64_t per_block) {
   const uint64_t want = (items + per_block - 1) / per_block;
   return (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)ws->sm_count * std::min(per_sm, 8), want));
+}
+
+int grid_ms(const MsWorkspace* ws, const void* kernel, uint64_t items, uint64_t per_block) {
+  return grid_for(ws, ms_occupancy(kernel), items, per_block);
 }
 
 // Node slots of a pass graph.
@@ -595,6 +603,7 @@ template <int W>
 struct MsArgs {
   MsParams<W> base;    // level 0: writes FR[0], list[0], cnt[0]
   MsParams<W> par[2];  // par[L & 1] for level L
+  uint64_t    m;       // out-edges of the pass's graph (bounds its frontier lists)
 };
 
 template <int W>
@@ -602,6 +611,7 @@ MsArgs<W> ms_args(GraphDev* g, MsWorkspace* ws, uint8_t* depth_rows, uint32_t k)
   MsArgs<W>    a;
   MsParams<W>& p = a.base;
   std::memset(&p, 0, sizeof p);
+  a.m        = g->m;
   p.off      = g->off;
   p.col      = g->col;
   p.in_off   = g->in_off;
@@ -667,12 +677,14 @@ cudaKernelNodeParams ms_node_params(MsWorkspace* ws, MsArgs<W>& a, int slot, voi
   if (slot == kNRoots) kp.gridDim = dim3(1);
   else if (slot == kNList) kp.gridDim = dim3(1);
   else {
-    int& cached = ws->node_grid[W - 1][slot];  // occupancy queried once per workspace
-    if (!cached)
-      cached = (slot == kNPush0 || slot == kNPush1) ? grid_ms(ws, kp.func, ws->list_cap, kMsWarps)
-               : slot == kNDepths ? grid_ms(ws, kp.func, (ws->n_cap + 63) / 64 * W, kMsWarps)
-                                  : grid_ms(ws, kp.func, ws->n_cap, kMsThreads);
-    kp.gridDim = dim3(cached);
+    // grids fit the pass's own graph (a workspace may be sized for a much
+    // larger one, as a serving slot's is); occupancy is queried once
+    int& per_sm = ws->node_occ[W - 1][slot];
+    if (!per_sm) per_sm = ms_occupancy(kp.func);
+    const uint64_t n = a.base.n;
+    kp.gridDim = dim3((slot == kNPush0 || slot == kNPush1) ? grid_for(ws, per_sm, n + a.m / kMsChunk + 1, kMsWarps)
+                      : slot == kNDepths                   ? grid_for(ws, per_sm, (n + 63) / 64 * W, kMsWarps)
+                                                           : grid_for(ws, per_sm, n, kMsThreads));
   }
   return kp;
 }
