@@ -172,8 +172,8 @@ struct MsWorkspace {
   void*           pass_host = nullptr;  // pinned staging of the same record
   cudaGraphExec_t exec[4] = {nullptr, nullptr, nullptr, nullptr};  // pass graphs, one per word count W
   cudaGraph_t     tmpl[4] = {nullptr, nullptr, nullptr, nullptr};  // their templates (own the nodes below)
-  cudaGraphNode_t nodes[4][9] = {};                                // kernel nodes updated per pass
-  int             node_occ[4][9] = {};                             // their resident blocks per SM
+  cudaGraphNode_t nodes[4][10] = {};                                // kernel nodes updated per pass
+  int             node_occ[4][10] = {};                             // their resident blocks per SM
   bool            stepped = false;      // host-driven levels (NWG_MS_STEPPED=1), for profilers
   cudaStream_t    stream  = nullptr;
   cudaEvent_t     ev0 = nullptr, ev1 = nullptr;

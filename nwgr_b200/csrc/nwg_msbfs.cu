@@ -529,11 +529,14 @@ __global__ void k_ms_root_list(MsParams<W> p) {  // level 0: writes list[0] and 
 // when the frontier's out-edges exceed the unpushed edges / alpha
 // (nw::graph::bfs, bfs.hpp:186), push otherwise.  Records the per-level
 // trace; with set_cond it drives the graph's WHILE node and this parity's
-// SWITCH node.  Once stopped, later calls only keep the loop stopped.
+// SWITCH node.  The call that stops the loop selects the depth rows (which
+// also clear the level planes, so they must run exactly once); later calls
+// only keep the loop stopped.
 __global__ void k_ms_decide(MsPassDev* d, cudaGraphConditionalHandle h_loop, cudaGraphConditionalHandle h_sw,
                             int set_cond) {
   if (threadIdx.x != 0) return;
-  bool stop = d->stopped != 0;
+  const bool was_stopped = d->stopped != 0;
+  bool       stop        = was_stopped;
   if (!stop) {
     const uint32_t    L    = d->level + 1;
     const MsCounters& prev = d->cnt[(L - 1) & 1];
@@ -568,8 +571,8 @@ __global__ void k_ms_decide(MsPassDev* d, cudaGraphConditionalHandle h_loop, cud
       d->level = L;
     }
   }
-  if (set_cond) {
-    cudaGraphSetConditional(h_sw, stop ? 2u : d->pull);
+  if (set_cond) {  // switch 2: the depth rows, once; 3: no branch
+    cudaGraphSetConditional(h_sw, stop ? (was_stopped ? 3u : 2u) : d->pull);
     cudaGraphSetConditional(h_loop, stop ? 0u : 1u);
   }
 }
@@ -596,7 +599,7 @@ int grid_ms(const MsWorkspace* ws, const void* kernel, uint64_t items, uint64_t 
 }
 
 // Node slots of a pass graph.
-enum { kNRoots, kNList, kNPush0, kNFin0, kNPull0, kNPush1, kNFin1, kNPull1, kNDepths, kNNodes };
+enum { kNRoots, kNList, kNPush0, kNFin0, kNPull0, kNPush1, kNFin1, kNPull1, kNDepths0, kNDepths1, kNNodes };
 
 // Arguments of a pass: the base set (roots, level 0) and the two parities.
 template <int W>
@@ -656,14 +659,15 @@ void* ms_node_fn(int slot) {
     case kNPush1: return (void*)k_ms_push<W>;
     case kNFin0:
     case kNFin1: return (void*)k_ms_finalize<W>;
-    case kNDepths: return (void*)k_ms_depths<W>;
+    case kNDepths0:
+    case kNDepths1: return (void*)k_ms_depths<W>;
     default: return (void*)k_ms_pull<W>;
   }
 }
 
 template <int W>
 MsParams<W>* ms_node_args(MsArgs<W>& a, int slot) {
-  if (slot == kNRoots || slot == kNList || slot == kNDepths) return &a.base;
+  if (slot == kNRoots || slot == kNList || slot == kNDepths0 || slot == kNDepths1) return &a.base;
   return slot < kNPush1 ? &a.par[1] : &a.par[0];  // the first half of the body runs odd levels
 }
 
@@ -683,16 +687,20 @@ cudaKernelNodeParams ms_node_params(MsWorkspace* ws, MsArgs<W>& a, int slot, voi
     if (!per_sm) per_sm = ms_occupancy(kp.func);
     const uint64_t n = a.base.n;
     kp.gridDim = dim3((slot == kNPush0 || slot == kNPush1) ? grid_for(ws, per_sm, n + a.m / kMsChunk + 1, kMsWarps)
-                      : slot == kNDepths                   ? grid_for(ws, per_sm, (n + 63) / 64 * W, kMsWarps)
+                      : slot >= kNDepths0                  ? grid_for(ws, per_sm, (n + 63) / 64 * W, kMsWarps)
                                                            : grid_for(ws, per_sm, n, kMsThreads));
   }
   return kp;
 }
 
 // The pass as a CUDA graph: roots, first frontier list, then
-// WHILE(decide -> SWITCH{push + finalize | pull} for an odd level, the same
-// for the following even level), then the depth rows; no host round trip
-// per level.
+// WHILE(decide -> SWITCH{push + finalize | pull | depth rows} for an odd
+// level, the same for the following even level); no host round trip per
+// level.  The decide that stops the loop selects the depth-rows branch of
+// its own switch, so the WHILE node stays the graph's last node.  The depth
+// kernel after the WHILE node, or launched on the stream after the graph,
+// made every pass of a 16-slot serving mix markedly slower (p99 at 50k
+// queries/s 13-14 ms against 8 ms with the branch).
 template <int W>
 int ms_build_exec(MsWorkspace* ws, MsArgs<W>& a) {
   MsPassDev*  d = static_cast<MsPassDev*>(ws->pass_dev);
@@ -740,16 +748,16 @@ int ms_build_exec(MsWorkspace* ws, MsArgs<W>& a) {
     sp.type                = cudaGraphNodeTypeConditional;
     sp.conditional.handle  = h_sw[half];
     sp.conditional.type    = cudaGraphCondTypeSwitch;
-    sp.conditional.size    = 2;
+    sp.conditional.size    = 3;
     if ((e = cudaGraphAddNode(&n_sw, body, &n_dec, 1, &sp)) != cudaSuccess) return fail(e, "switch node");
     const int push = half == 0 ? kNPush0 : kNPush1;
     if ((e = add(sp.conditional.phGraph_out[0], nullptr, push)) != cudaSuccess ||
         (e = add(sp.conditional.phGraph_out[0], &nodes[push], push + 1)) != cudaSuccess ||
-        (e = add(sp.conditional.phGraph_out[1], nullptr, push + 2)) != cudaSuccess)
+        (e = add(sp.conditional.phGraph_out[1], nullptr, push + 2)) != cudaSuccess ||
+        (e = add(sp.conditional.phGraph_out[2], nullptr, kNDepths0 + half)) != cudaSuccess)
       return fail(e, "level nodes");
     prev = n_sw;
   }
-  if ((e = add(graph, &n_while, kNDepths)) != cudaSuccess) return fail(e, "depth rows node");
   cudaGraphExec_t exec;
   if ((e = cudaGraphInstantiate(&exec, graph, 0)) != cudaSuccess) return fail(e, "multi-source graph instantiate");
   if (ws->tmpl[W - 1]) cudaGraphDestroy(ws->tmpl[W - 1]);
