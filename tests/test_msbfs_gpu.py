@@ -62,3 +62,49 @@ def test_msbfs_rmat20_device_graph(nwg, port):
     assert np.array_equal(d[sample], want)
     assert st.push_levels > 0 and st.pull_levels > 0
     g.release()
+
+
+def test_msbfs_odd_n_and_unaligned_rows(nwg, port):
+    """An odd vertex count and a depth array that starts at an odd address:
+    the depth rows are then written byte by byte, and every byte of every
+    row must still be right, with nothing written outside the rows."""
+    import torch
+
+    off, cols = gg.grid(61, 49, 1, seed=7)  # n = 2989
+    n = off.size - 1
+    g = nwg.Graph.from_csr(off, cols)
+    ws = nwg.MsWorkspace(g)
+    for k in (7, 70):
+        roots = gg.roots(off, k, seed=k)
+        buf = torch.full((k * n + 2,), 7, dtype=torch.uint8, device="cuda")
+        ws.run(roots, buf[1 : 1 + k * n])
+        h = buf.cpu().numpy()
+        assert h[0] == 7 and h[-1] == 7
+        assert np.array_equal(h[1:-1].reshape(k, n), port.msbfs_depths(off, cols, roots))
+    ws.close()
+    g.release()
+
+
+def test_msbfs_workspace_reuse_after_deep_and_overflowing_passes(nwg, port):
+    """One workspace, passes in a row on a 400-vertex path: depths up to 253
+    (all eight level planes), passes that stop on a depth overflow, and
+    passes after them.  The planes must be clear again after each pass."""
+    import torch
+
+    n = 400
+    u = np.arange(n - 1, dtype=np.uint64)
+    off, cols = gg.csr_from_pairs(u, u + np.uint64(1), n)
+    g = nwg.Graph.from_csr(off, cols)
+    ws = nwg.MsWorkspace(g)
+    d = torch.empty((2, n), dtype=torch.uint8, device="cuda")
+    for roots in ([200, 150], [0, 5], [180, 253], [230, 146], [3, 399]):
+        roots = np.asarray(roots, np.uint32)
+        if max(max(int(r), n - 1 - int(r)) for r in roots) >= 254:  # a level 255 would have to be tried
+            with pytest.raises(nwg.NwgError) as e:
+                ws.run(roots, d)
+            assert e.value.code == nwg.NWG_EOVERFLOW
+            continue
+        ws.run(roots, d)
+        assert np.array_equal(d.cpu().numpy(), port.msbfs_depths(off, cols, roots))
+    ws.close()
+    g.release()
