@@ -32,6 +32,11 @@ project's TBB-compatible thread pool, oracle/_ref) on this host's cores,
 timed like bench/common.hpp's time_op, on a bounded sample of the roots.
 
 Further sections of the same JSON line (each skippable with --no-<name>):
+  other        the other graphs of the single-source workload (of RMAT-24,
+               uniform 2^24 with average degree 32, the 4096 x 4096 grid with
+               1% shortcuts, those not named by --graph): GTEPS over 16 roots
+               timed like the main line, roofline fraction, and the
+               reference's bfs on the host for one root
   verifier     device BFSVerifier time per root, and the reference's
                verifier on the host for the first root
   batched      multi-source BFS on RMAT-22 with 64/256/1024 roots against 64
@@ -89,6 +94,7 @@ def parse():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-verify", action="store_true")
     ap.add_argument("--no-bc", action="store_true")
+    ap.add_argument("--no-other", action="store_true", help="skip the other graphs of the single-source workload")
     ap.add_argument("--profile-msbfs", action="store_true",
                     help="one multi-source pass on RMAT-22 (--ms-sources roots), levels driven from the host, in "
                          "NVTX range nwg_profile (for ncu)")
@@ -487,6 +493,65 @@ def bench_serving(nwg, num_graphs=200, rates=SERVE_RATES, seconds=1.5, slots=16,
             "generate_s": gen_s, "rates": out}
 
 
+def bench_other_graphs(nwg, torch, main_graph, hbm, with_cpu, n_roots=16, reps=3):
+    """The other graphs of the single-source workload (RMAT-24, uniform 2^24
+    at average degree 32, the 4096 x 4096 grid with 1% shortcuts), each
+    timed like the main line: device time per traversal with the L2 flushed
+    before it, GTEPS as the harmonic mean over `n_roots` roots, algorithmic
+    bytes over time against the HBM peak; beside it the reference's bfs on
+    the host for the first root."""
+    out = {}
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for name in ("rmat24", "uniform24", "grid4096"):
+        if name == main_graph:
+            continue
+        spec = graph_spec(name)
+        g = make_graph(nwg, spec)
+        roots = g.roots(n_roots, seed=ROOT_SEED)
+        ws = g.workspace()
+        par = torch.empty(g.n, dtype=torch.int32, device="cuda")
+        stream = torch.cuda.Stream()
+        e_r, n_r = [], []
+        for r in roots:
+            with torch.cuda.stream(stream):
+                ws.bfs_async(int(r), par, stream.cuda_stream)
+            stream.synchronize()
+            e, v = g.component_edges(par)
+            e_r.append(e)
+            n_r.append(v)
+        e_r, n_r = np.asarray(e_r, np.float64), np.asarray(n_r, np.float64)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in roots]
+        times = []
+        for rep in range(reps + 1):
+            for i, r in enumerate(roots):
+                with torch.cuda.stream(stream):
+                    flush.fill_(i & 0xFF)
+                    ev[i][0].record(stream)
+                    ws.bfs_async(int(r), par, stream.cuda_stream)
+                    ev[i][1].record(stream)
+            stream.synchronize()
+            if rep:  # the first round is warm-up
+                times.append([ev[i][0].elapsed_time(ev[i][1]) for i in range(len(roots))])
+        t = np.mean(np.asarray(times), axis=0)
+        gteps = (e_r / 2.0) / (t * 1e-3) / 1e9
+        b_r = 4.0 * e_r + 8.0 * n_r + 4.0 * g.n
+        achieved = float(np.mean(b_r / (t * 1e-3)) / 1e9)
+        st = ws.stats()
+        row = {"workload": workload_name(spec), "n": g.n, "m_directed": g.m, "roots": int(roots.size),
+               "gteps": hmean(gteps), "ms_per_root_median": float(np.median(t)), "levels_last_root": int(st.levels),
+               "roofline": {"achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm}}
+        ws.close()
+        if with_cpu:
+            off, cols = g.csr()
+            g.release()
+            row["cpu_reference"] = cpu_baseline(off, cols, roots, 1)
+            del off, cols
+        else:
+            g.release()
+        out[name] = row
+    return out
+
+
 def cpu_baseline(off, cols, roots, n_roots):
     """Reference bfs.hpp on the host cores over a bounded sample of roots."""
     from oracle.oracle import Reference
@@ -638,11 +703,19 @@ def main():
     verifier = None
     if not args.no_verify:
         verifier = bench_verifier(nwg, torch, g, roots, rank == 0 and not args.no_cpu)
+    other = None
+    if not args.no_other and rank == 0:
+        if ws is not None:
+            ws.close()
+            g.release()
+            ws, g = None, None
+        other = bench_other_graphs(nwg, torch, args.graph, hbm, not args.no_cpu)
     batched = None
     if not args.no_batched:
-        ws.close()
-        g.release()
-        ws, g = None, None
+        if ws is not None:
+            ws.close()
+            g.release()
+            ws, g = None, None
         batched = bench_batched(nwg, torch)
     ragged = None
     if not args.no_ragged:
@@ -692,7 +765,7 @@ def main():
                                          "scaled by directed entries" if traffic else None},
             "gpu_launches": int(np.sum(launches)) * args.steps,
             "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, "batched": batched, "ragged": ragged,
-            "serving": serving, "verifier": verifier, "betweenness": bc,
+            "serving": serving, "verifier": verifier, "betweenness": bc, "other_graphs": other,
         }
         print(json.dumps(line), flush=True)
     if ws is not None:
