@@ -252,7 +252,9 @@ struct GraphDev {
   uint32_t* Z = nullptr;  // in-degree-zero bitmap
   bool      owns_out = false, owns_in = false, symmetric = true;
   int       sm_count = 148;
-  Thresholds th{32, 256, 8};
+  // out-degree >= 64 goes to the chunk queue: 2.0% (RMAT-24) and 2.4%
+  // (uniform 2^24) faster than 32 on a B200; 512-edge chunks gained nothing
+  Thresholds th{64, 256, 8};
   std::mutex                mu;
   Workspace*                default_ws = nullptr;
   std::vector<Workspace*>   workspaces;
