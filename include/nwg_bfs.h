@@ -163,9 +163,10 @@ int nwg_graph_copy_csr(nwg_graph g, uint64_t* out_off, uint32_t* out_col, uint64
  * uint8: depth of vertex v from root i at depths_dev[i * n + v], 255 =
  * unreached; NWG_EOVERFLOW if some depth would be >= 255.  Runs on `stream`
  * (NULL = the workspace's own stream) and returns when done.  A workspace
- * holds 384 * n bytes of device state (three bitsets and eight level
- * bit-planes of four 64-bit words per vertex) plus two frontier lists of
- * 8 * (n + m / 256 + 1) bytes: about 1.7 GB for RMAT-22, 6.7 GB for RMAT-24.
+ * holds about 388 * n bytes of device state (three bitsets and eight level
+ * bit-planes of four 64-bit words per vertex, a touched-vertex list and its
+ * bitmap) plus two frontier lists of 8 * (n + m / 256 + 1) bytes: about
+ * 1.7 GB for RMAT-22, 6.8 GB for RMAT-24.
  * Calls on one workspace must not overlap. */
 typedef struct nwg_msbfs_ws_s* nwg_msbfs_ws;
 #define NWG_MS_TRACE_CAP 64

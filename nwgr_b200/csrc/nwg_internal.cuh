@@ -166,6 +166,8 @@ struct MsWorkspace {
   uint64_t*       fr[2]   = {nullptr, nullptr};
   uint64_t*       nx      = nullptr;
   uint64_t*       dp      = nullptr;  // 8 level bit-planes (depth bit j of each source), zero between passes
+  uint32_t*       tlist   = nullptr;  // vertices a push level touched (sparse finalize)
+  uint32_t*       tbits   = nullptr;  // their bitmap, zero between levels
   uint64_t*       list[2] = {nullptr, nullptr};  // frontier chunk entries
   uint64_t        list_cap = 0;
   void*           pass_dev  = nullptr;  // arguments and level-loop state of a pass (device)

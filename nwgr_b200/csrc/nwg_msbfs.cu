@@ -41,6 +41,7 @@ struct MsCounters {
   unsigned long long frontier_edges;  // out-edges of the next frontier's vertices
   unsigned long long frontier_count;  // chunk entries in the next frontier list
   unsigned long long alive[4];        // sources with a vertex in the next frontier (their BFS goes on)
+  unsigned long long touched;         // push: vertices in the touched list (NX made non-zero)
 };
 
 constexpr uint32_t kMsChunk      = 256;  // out-edges per frontier chunk entry (one warp's push task)
@@ -61,6 +62,10 @@ struct MsPassDev {
   int32_t    status;
   uint32_t   levels;     // max depth + 1
   uint32_t   pull, stopped, push_levels, pull_levels, trace_len;
+  uint64_t   sparse_max;  // a push level finalizes only its touched vertices when it pushes at most this many edges
+  uint64_t   clear_max;   // ... and the frontier two levels back has at most this many chunk entries
+  uint64_t   nclear;      // chunk entries of the frontier two levels back (still in list_nxt)
+  uint32_t   sparse_ok;   // this push level finalizes sparsely
   MsCounters cnt[2];     // level L's kernels add into cnt[L & 1]
   uint32_t   roots[256], uniq[256];
   uint8_t    tr_pull[kMsTrace];
@@ -84,6 +89,8 @@ struct MsParams {
   uint64_t*        fr_nxt;
   uint64_t*        nx;
   uint64_t*        dp;        // level bit-planes, plane j at dp + j * plane
+  uint32_t*        tlist;     // vertices a push level touched (NX made non-zero), in touch order
+  uint32_t*        T;         // bitmap of those vertices (deduplicates the list); zero between levels
   uint64_t         plane;     // words per plane (n * W)
   uint64_t*        list_cur;  // frontier chunk entries (vertex << 32 | chunk), push input
   uint64_t*        list_nxt;
@@ -272,12 +279,33 @@ __device__ __forceinline__ void ms_seen_publish(const MsParams<W>& p, uint64_t (
 
 // Push: one warp per frontier chunk entry (up to kMsChunk out-edges of one
 // vertex), so hubs are spread over the grid; lanes stride over the edges.
+// On a level that finalizes sparsely (at most sparse_max edges pushed, at
+// most clear_max entries two levels back) it also
+//   * clears FR[nxt] of the frontier two levels back, whose chunk entries
+//     list_nxt still holds (this kernel reads neither FR[nxt] nor list_nxt);
+//     a frontier vertex without out-edges has no entry and keeps its stale
+//     word, which no kernel reads: a push reads the frontier words of list
+//     entries only, a pull those of in-neighbours, which have out-edges;
+//   * lists each vertex whose NX it makes non-zero, once (the T bitmap
+//     deduplicates).  The list cannot outgrow sparse_max; should a warp see
+//     more, it stops listing and the finalize sweeps every vertex.
 template <int W>
 __global__ void __launch_bounds__(kMsThreads) k_ms_push(MsParams<W> p) {
-  const uint64_t nlist = p.d->nlist;
+  const uint64_t nlist  = p.d->nlist;
+  const bool     sparse = p.d->sparse_ok != 0;
+  const uint64_t smax   = p.d->sparse_max;
   const unsigned lane   = threadIdx.x & 31;
   const uint64_t gwarp  = (uint64_t)blockIdx.x * kMsWarps + (threadIdx.x >> 5);
   const uint64_t nwarps = (uint64_t)gridDim.x * kMsWarps;
+  if (sparse) {
+    const uint64_t nclear = p.d->nclear;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nclear; i += stride) {
+      const uint64_t u = p.list_nxt[i] >> 32;
+#pragma unroll
+      for (int w = 0; w < W; ++w) p.fr_nxt[u * W + w] = 0;
+    }
+  }
   for (uint64_t i = gwarp; i < nlist; i += nwarps) {
     const uint64_t ent = p.list_cur[i];
     const uint32_t u   = (uint32_t)(ent >> 32);
@@ -285,14 +313,41 @@ __global__ void __launch_bounds__(kMsThreads) k_ms_push(MsParams<W> p) {
     ms_words<W>(p.fr_cur + (uint64_t)u * W, f);
     const uint64_t beg = p.off[u] + ((ent & 0xFFFFFFFFull) << kMsChunkShift);
     const uint64_t end = min(p.off[u + 1], beg + kMsChunk);
-    for (uint64_t e = beg + lane; e < end; e += 32) {
-      const uint32_t v = __ldg(p.col + e);
-      uint64_t       seen[W];
-      ms_words<W>(p.vis + (uint64_t)v * W, seen);  // VIS is stable during the push
+    unsigned long long seen_count = 0;
+    if (sparse && lane == 0) seen_count = *(volatile unsigned long long*)&p.cnt->touched;
+    const bool track = sparse && __shfl_sync(kFullMask, seen_count, 0) <= smax;  // warp-uniform
+    for (uint64_t base = beg; base < end; base += 32) {
+      const uint64_t e     = base + lane;
+      bool           first = false;  // this lane made one of v's NX words non-zero
+      uint32_t       v     = 0;
+      if (e < end) {
+        v = __ldg(p.col + e);
+        uint64_t seen[W];
+        ms_words<W>(p.vis + (uint64_t)v * W, seen);  // VIS is stable during the push
 #pragma unroll
-      for (int w = 0; w < W; ++w) {
-        const uint64_t m = f[w] & ~seen[w];
-        if (m) atomicOr((unsigned long long*)&p.nx[(uint64_t)v * W + w], (unsigned long long)m);
+        for (int w = 0; w < W; ++w) {
+          const uint64_t m = f[w] & ~seen[w];
+          if (!m) continue;
+          if (track) {  // the old value is needed only here: elsewhere the OR stays a fire-and-forget reduction
+            if (atomicOr((unsigned long long*)&p.nx[(uint64_t)v * W + w], (unsigned long long)m) == 0ull) first = true;
+          } else {
+            atomicOr((unsigned long long*)&p.nx[(uint64_t)v * W + w], (unsigned long long)m);
+          }
+        }
+      }
+      if (track) {
+        const uint32_t bit = 1u << (v & 31);
+        const bool     add = first && !(atomicOr(&p.T[v >> 5], bit) & bit);
+        const unsigned am  = __ballot_sync(kFullMask, add);
+        if (am) {
+          unsigned long long b = 0;
+          if (lane == 0) b = atomicAdd(&p.cnt->touched, (unsigned long long)__popc(am));
+          b = __shfl_sync(kFullMask, b, 0);
+          if (add) {
+            const unsigned long long pos = b + __popc(am & ((1u << lane) - 1u));
+            if (pos < p.n) p.tlist[pos] = v;
+          }
+        }
       }
     }
   }
@@ -335,8 +390,40 @@ __device__ __forceinline__ void ms_append(const MsParams<W>& p, bool has, uint32
   }
 }
 
-// Finalize after a push: NX -> new bits, VIS, FR[nxt], depths, next list.
-// Every vertex's FR[nxt] words are written (zero when nothing is new).
+// One vertex of a finalize: NX -> new bits, VIS, FR[nxt], level planes,
+// next list.  All 32 lanes of the warp call it (valid false for padding).
+template <int W>
+__device__ __forceinline__ void finalize_vertex(const MsParams<W>& p, uint32_t level, bool valid, uint64_t v,
+                                                unsigned long long& disc, unsigned long long& fedges,
+                                                uint64_t (&seen_slot)[4]) {
+  uint64_t nw[W];
+  bool     has = false;
+#pragma unroll
+  for (int w = 0; w < W; ++w) {
+    nw[w] = 0;
+    if (valid) {
+      const uint64_t x = p.nx[v * W + w];
+      if (x) {
+        const uint64_t vis = p.vis[v * W + w];
+        nw[w]              = x & ~vis;
+        p.nx[v * W + w]    = 0;
+        if (nw[w]) p.vis[v * W + w] = vis | nw[w];
+      }
+      p.fr_nxt[v * W + w] = nw[w];
+      has |= nw[w] != 0;
+      disc += __popcll(nw[w]);
+    }
+  }
+  if (has) record_level<W>(p, level, v, nw);
+  ms_seen_add<W>(seen_slot, nw);
+  ms_append<W>(p, has, (uint32_t)v, fedges, has ? (unsigned long long)(p.off[v + 1] - p.off[v]) : 0ull);
+}
+
+// Finalize after a push.  Sparse when the push listed every vertex it
+// touched and cleared FR[nxt] of the frontier two levels back: only the listed vertices are visited, every other FR[nxt]
+// word is already zero (or stale for a vertex no kernel reads).  Otherwise
+// every vertex's FR[nxt] words are written (zero when nothing is new).
+// Either way the T bits the push set are cleared.
 template <int W>
 __global__ void __launch_bounds__(kMsThreads) k_ms_finalize(MsParams<W> p) {
   const uint32_t level = p.d->level;
@@ -344,31 +431,24 @@ __global__ void __launch_bounds__(kMsThreads) k_ms_finalize(MsParams<W> p) {
   __shared__ uint64_t s_seen[kMsWarps][4];
   if ((threadIdx.x & 31) < 4) s_seen[threadIdx.x >> 5][threadIdx.x & 31] = 0;
   __syncwarp();
-  const uint64_t     stride = (uint64_t)gridDim.x * blockDim.x;
-  const uint64_t     n_up   = (p.n + 31) & ~31ull;
-  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n_up; v += stride) {
-    const bool valid = v < p.n;
-    uint64_t   nw[W];
-    bool       has = false;
-#pragma unroll
-    for (int w = 0; w < W; ++w) {
-      nw[w] = 0;
-      if (valid) {
-        const uint64_t x = p.nx[v * W + w];
-        if (x) {
-          const uint64_t vis = p.vis[v * W + w];
-          nw[w]              = x & ~vis;
-          p.nx[v * W + w]    = 0;
-          if (nw[w]) p.vis[v * W + w] = vis | nw[w];
-        }
-        p.fr_nxt[v * W + w] = nw[w];
-        has |= nw[w] != 0;
-        disc += __popcll(nw[w]);
-      }
+  const uint64_t     stride  = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t     touched = p.cnt->touched;
+  const bool         sparse  = p.d->sparse_ok != 0 && touched <= p.d->sparse_max;
+  if (sparse) {
+    const uint64_t t_up = (touched + 31) & ~31ull;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < t_up; i += stride) {
+      const bool     valid = i < touched;
+      const uint64_t v     = valid ? p.tlist[i] : 0;
+      if (valid) p.T[v >> 5] = 0;
+      finalize_vertex<W>(p, level, valid, v, disc, fedges, s_seen[threadIdx.x >> 5]);
     }
-    if (has) record_level<W>(p, level, v, nw);
-    ms_seen_add<W>(s_seen[threadIdx.x >> 5], nw);
-    ms_append<W>(p, has, (uint32_t)v, fedges, has ? (unsigned long long)(p.off[v + 1] - p.off[v]) : 0ull);
+  } else {
+    const uint64_t n_up = (p.n + 31) & ~31ull;
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n_up; v += stride) {
+      const bool valid = v < p.n;
+      if (valid && (v & 31) == 0) p.T[v >> 5] = 0;
+      finalize_vertex<W>(p, level, valid, v, disc, fedges, s_seen[threadIdx.x >> 5]);
+    }
   }
   ms_seen_publish<W>(p, s_seen);
   const unsigned long long dsum = ms_block_sum(disc);
@@ -558,8 +638,13 @@ __global__ void k_ms_decide(MsPassDev* d, cudaGraphConditionalHandle h_loop, cud
     } else {
       const uint64_t fedges = prev.frontier_edges;
       d->nlist              = min((uint64_t)prev.frontier_count, d->list_cap);
+      // list[L & 1] still holds the chunk entries of level L - 2's frontier
+      const uint64_t old    = min((uint64_t)d->cnt[L & 1].frontier_count, d->list_cap);
       d->cnt[L & 1]         = MsCounters{};
       const bool pull       = fedges > d->unchecked / (uint64_t)d->alpha;
+      d->nclear             = old;
+      // the push touches at most fedges vertices, so a sparse level's list never overflows
+      d->sparse_ok          = (!pull && fedges <= d->sparse_max && old <= d->clear_max) ? 1u : 0u;
       if (!pull) d->unchecked -= min(d->unchecked, fedges);
       if (L - 1 < kMsTrace) {
         d->tr_pull[L - 1]   = pull ? 1 : 0;
@@ -624,6 +709,8 @@ MsArgs<W> ms_args(GraphDev* g, MsWorkspace* ws, uint8_t* depth_rows, uint32_t k)
   p.vis      = ws->vis;
   p.nx       = ws->nx;
   p.dp       = ws->dp;
+  p.tlist    = ws->tlist;
+  p.T        = ws->tbits;
   p.plane    = g->n * W;
   p.list_cap = ws->list_cap;
   p.depth    = depth_rows;
@@ -844,6 +931,8 @@ int ms_pass(GraphDev* g, MsWorkspace* ws, const uint32_t* roots_host, uint32_t k
   h.k         = k;
   h.alpha     = alpha;
   h.unchecked = g->m;
+  h.sparse_max = std::max<uint64_t>(1024, n / 64);
+  h.clear_max  = std::max<uint64_t>(1024, n / 8);
   std::memcpy(h.roots, roots_host, k * sizeof(uint32_t));
   // distinct roots form the first frontier; their chunk entries the first list
   std::vector<uint32_t> uniq(roots_host, roots_host + k);
@@ -856,6 +945,7 @@ int ms_pass(GraphDev* g, MsWorkspace* ws, const uint32_t* roots_host, uint32_t k
   const size_t words = (size_t)n * W * sizeof(uint64_t);
   NWG_CUDA_TRY(cudaMemsetAsync(ws->vis, 0, words, stream));
   NWG_CUDA_TRY(cudaMemsetAsync(ws->fr[0], 0, words, stream));
+  NWG_CUDA_TRY(cudaMemsetAsync(ws->fr[1], 0, words, stream));  // a sparse first level writes only what it touches
   NWG_CUDA_TRY(cudaMemsetAsync(ws->nx, 0, words, stream));
   NWG_CUDA_TRY(cudaMemcpyAsync(dd, &h, sizeof h, cudaMemcpyHostToDevice, stream));
   if (ws->stepped) {
@@ -893,7 +983,9 @@ uint64_t ms_ws_bytes(uint64_t n_cap, uint64_t m_cap) {
   // VIS, FR[2], NX and the 8 level planes at four words per vertex, two
   // frontier lists (every frontier vertex has at most deg / kMsChunk + 1
   // entries), the pass record
-  return (4 + kMsPlanes) * n * 4 * sizeof(uint64_t) + 2 * (n + m_cap / kMsChunk + 1) * 8 + sizeof(MsPassDev);
+  // plus the touched list and its bitmap
+  return (4 + kMsPlanes) * n * 4 * sizeof(uint64_t) + 2 * (n + m_cap / kMsChunk + 1) * 8 + sizeof(MsPassDev) +
+         4 * n + 4 * (n / 32 + 1);
 }
 
 int ms_ws_init_cap(GraphDev* g, uint64_t n_cap, uint64_t m_cap, MsWorkspace* ws) {
@@ -912,6 +1004,8 @@ int ms_ws_init_cap(GraphDev* g, uint64_t n_cap, uint64_t m_cap, MsWorkspace* ws)
   if (cudaMalloc(&ws->vis, words) != cudaSuccess || cudaMalloc(&ws->fr[0], words) != cudaSuccess ||
       cudaMalloc(&ws->fr[1], words) != cudaSuccess || cudaMalloc(&ws->nx, words) != cudaSuccess ||
       cudaMalloc(&ws->dp, kMsPlanes * words) != cudaSuccess ||
+      cudaMalloc(&ws->tlist, n * sizeof(uint32_t)) != cudaSuccess ||
+      cudaMalloc(&ws->tbits, (n / 32 + 1) * sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(&ws->list[0], list_cap * 8) != cudaSuccess || cudaMalloc(&ws->list[1], list_cap * 8) != cudaSuccess ||
       cudaMalloc(&ws->pass_dev, sizeof(MsPassDev)) != cudaSuccess ||
       cudaMallocHost(&ws->pass_host, sizeof(MsPassDev)) != cudaSuccess) {
@@ -919,6 +1013,7 @@ int ms_ws_init_cap(GraphDev* g, uint64_t n_cap, uint64_t m_cap, MsWorkspace* ws)
     return set_error(NWG_ENOMEM, "multi-source workspace allocation failed");
   }
   NWG_CUDA_TRY(cudaMemset(ws->dp, 0, kMsPlanes * words));  // the planes start (and end every pass) zero
+  NWG_CUDA_TRY(cudaMemset(ws->tbits, 0, (n / 32 + 1) * sizeof(uint32_t)));  // so does T (every finalize clears it)
   NWG_CUDA_TRY(cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking));
   NWG_CUDA_TRY(cudaEventCreate(&ws->ev0));
   NWG_CUDA_TRY(cudaEventCreate(&ws->ev1));
@@ -946,6 +1041,8 @@ void ms_ws_free(MsWorkspace* ws) {
   cudaFree(ws->fr[1]);
   cudaFree(ws->nx);
   cudaFree(ws->dp);
+  cudaFree(ws->tlist);
+  cudaFree(ws->tbits);
   cudaFree(ws->list[0]);
   cudaFree(ws->list[1]);
   cudaFree(ws->pass_dev);
