@@ -530,7 +530,7 @@ def bench_other_graphs(nwg, torch, main_graph, hbm, with_cpu, n_roots=16, reps=3
                     ws.bfs_async(int(r), par, stream.cuda_stream)
                     ev[i][1].record(stream)
             stream.synchronize()
-            if rep:  # the first round is warm-up
+            if rep:  # the first pass over the roots is warm-up
                 times.append([ev[i][0].elapsed_time(ev[i][1]) for i in range(len(roots))])
         t = np.mean(np.asarray(times), axis=0)
         gteps = (e_r / 2.0) / (t * 1e-3) / 1e9
