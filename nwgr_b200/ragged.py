@@ -16,8 +16,10 @@ changes); per batch it chooses the resident blocks per SM of the persistent
 launch.  Choices are timed on the device (CUDA events of the persistent
 launch) over a sample of each class's items.
 
-Cache: JSON at $NWG_AUTOTUNE_CACHE, else nwgr_b200/autotune_cache.json,
-keyed by GPU name and library version.
+Cache: JSON at $NWG_AUTOTUNE_CACHE, else $XDG_CACHE_HOME/nwgr_b200/autotune.json
+(~/.cache when XDG_CACHE_HOME is unset), keyed by GPU name and library
+version.  Tuning results belong to the machine that measured them, so the
+package ships none: a class the cache lacks is tuned on first use.
 """
 from __future__ import annotations
 
@@ -30,8 +32,12 @@ import numpy as np
 
 from . import RaggedBatch, version
 
-HERE = os.path.dirname(os.path.abspath(__file__))
-DEFAULT_CACHE = os.path.join(HERE, "autotune_cache.json")
+
+
+def default_cache_path() -> str:
+    base = os.environ.get("XDG_CACHE_HOME") or os.path.join(os.path.expanduser("~"), ".cache")
+    return os.path.join(base, "nwgr_b200", "autotune.json")
+
 
 WARP_MIN = (32, 64, 128)
 ALPHA = (15, 60)
@@ -63,7 +69,7 @@ def _device_key() -> str:
 
 class Autotuner:
     def __init__(self, path: str | None = None):
-        self.path = path or os.environ.get("NWG_AUTOTUNE_CACHE", DEFAULT_CACHE)
+        self.path = path or os.environ.get("NWG_AUTOTUNE_CACHE") or default_cache_path()
         self.key = _device_key()
         self.cache = {}
         try:
@@ -75,6 +81,7 @@ class Autotuner:
 
     def save(self) -> None:
         try:
+            os.makedirs(os.path.dirname(os.path.abspath(self.path)), exist_ok=True)
             tmp = self.path + ".tmp"
             with open(tmp, "w") as f:
                 json.dump(self.cache, f, indent=1, sort_keys=True)

@@ -22,13 +22,73 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_SO = os.path.join(HERE, "_build", "libnwgport.so")
 REF_SO = os.path.join(HERE, "_ref", "libnwgref.so")
-REFERENCE_INCLUDE = os.environ.get("NWG_REFERENCE_INCLUDE", "/root/reference/include")
+# NWGraph's source tree: $NWG_REFERENCE_ROOT, else a checkout named
+# "reference" beside this repository (its include/ holds nwgraph/).
+REFERENCE_ROOT = os.environ.get("NWG_REFERENCE_ROOT",
+                                os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
+REFERENCE_INCLUDE = os.environ.get("NWG_REFERENCE_INCLUDE", os.path.join(REFERENCE_ROOT, "include"))
 NULLV = 0xFFFFFFFF
 
 _u64p = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
 _u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
 _u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
 _f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+
+
+GEN_SO = os.path.join(HERE, "_build", "libnwggen.so")
+KIND_RMAT, KIND_UNIFORM, KIND_GRID = 0, 1, 2
+
+
+def build_gen(force: bool = False) -> str:
+    src = os.path.join(HERE, "graphgen_host.c")
+    if force or not os.path.exists(GEN_SO) or os.path.getmtime(GEN_SO) < os.path.getmtime(src):
+        os.makedirs(os.path.dirname(GEN_SO), exist_ok=True)
+        subprocess.check_call(["gcc", "-O3", "-std=c11", "-fPIC", "-shared", "-fopenmp", src, "-o", GEN_SO + ".tmp"])
+        os.replace(GEN_SO + ".tmp", GEN_SO)
+    return GEN_SO
+
+
+class HostGen:
+    """ctypes view of oracle/graphgen_host.c: the seeded generators of
+    oracle/graphgen.py built on the host cores (OpenMP).  Same graphs, bit
+    for bit, in seconds at scale 24."""
+
+    def __init__(self, threads: int = 0):
+        lib = C.CDLL(build_gen())
+        lib.nwggen_capacity.restype = C.c_uint64
+        lib.nwggen_capacity.argtypes = [C.c_int, C.c_uint64, C.c_uint64, C.c_uint64]
+        lib.nwggen_vertices.restype = C.c_uint64
+        lib.nwggen_vertices.argtypes = [C.c_int, C.c_uint64, C.c_uint64, C.c_uint64]
+        lib.nwggen_csr.restype = C.c_int64
+        lib.nwggen_csr.argtypes = [C.c_int, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint32,
+                                   C.c_uint32, C.c_int, _u64p, _u32p, _u32p, C.c_uint64]
+        self.lib = lib
+        self.threads = int(threads)
+
+    def _csr(self, kind, a0, a1, a2, seed, thr=(0, 0, 0)):
+        cap = int(self.lib.nwggen_capacity(kind, a0, a1, a2))
+        n = int(self.lib.nwggen_vertices(kind, a0, a1, a2))
+        if cap == 0 and n == 0:
+            raise ValueError("bad generator arguments")
+        off = np.empty(n + 1, np.uint64)
+        tmp = np.empty(max(cap, 1), np.uint32)
+        cols = np.empty(max(cap, 1), np.uint32)
+        m = self.lib.nwggen_csr(kind, a0, a1, a2, seed & 0xFFFFFFFFFFFFFFFF, *thr, self.threads, off, tmp, cols, cap)
+        if m < 0:
+            raise ValueError(f"nwggen_csr failed: {m}")
+        del tmp
+        return off, (cols[:m].copy() if m < cap // 2 else cols[:m])
+
+    def rmat(self, scale: int, edge_factor: int = 16, seed: int = 1, a=0.57, b=0.19, c=0.19):
+        from oracle.graphgen import rmat_thresholds
+
+        return self._csr(KIND_RMAT, scale, edge_factor, 0, seed, rmat_thresholds(a, b, c))
+
+    def uniform(self, n: int, avg_degree: int = 32, seed: int = 1):
+        return self._csr(KIND_UNIFORM, n, avg_degree, 0, seed)
+
+    def grid(self, width: int, height: int, shortcut_pct: int = 1, seed: int = 1):
+        return self._csr(KIND_GRID, width, height, shortcut_pct, seed)
 
 
 def build_port(force: bool = False) -> str:

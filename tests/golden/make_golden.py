@@ -2,7 +2,8 @@
 
 Run where the NWGraph sources exist (they are read, never copied):
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py [--reference PATH]   (default: $NWG_REFERENCE_ROOT, else a
+    checkout named "reference" beside this repository)
 
 For every MatrixMarket fixture in the reference's data/ directory the script
 builds the edge set exactly as read_mm does (io/mmio.hpp:86-103,172-208:
@@ -47,9 +48,10 @@ def csr_keep_all(u, v, n):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=None, help="NWGraph source tree")
     ap.add_argument("--out", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "fixtures.npz"))
     args = ap.parse_args()
+    args.reference = args.reference or O.REFERENCE_ROOT
     os.environ["NWG_REFERENCE_INCLUDE"] = os.path.join(args.reference, "include")
     O.REFERENCE_INCLUDE = os.environ["NWG_REFERENCE_INCLUDE"]
     ref = O.Reference()

@@ -2,7 +2,8 @@
 
 Run where the NWGraph sources exist (they are compiled, never copied):
 
-    python tests/golden/make_nwbin.py [--reference /root/reference]
+    python tests/golden/make_nwbin.py [--reference PATH]   (default: $NWG_REFERENCE_ROOT, else a
+    checkout named "reference" beside this repository)
 
 A small program, compiled against the unmodified NWGraph headers and the
 project's TBB-compatible shim (oracle/tbb_compat), reads MatrixMarket
@@ -82,8 +83,13 @@ FIXTURES = ("karate", "bktest2", "sherman4")  # symmetric, directed, directed wi
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=None, help="NWGraph source tree")
     args = ap.parse_args()
+    if args.reference is None:
+        sys.path.insert(0, ROOT)
+        from oracle.oracle import REFERENCE_ROOT
+
+        args.reference = REFERENCE_ROOT
     with tempfile.TemporaryDirectory() as tmp:
         src = os.path.join(tmp, "nwbin_writer.cpp")
         exe = os.path.join(tmp, "nwbin_writer")

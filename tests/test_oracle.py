@@ -142,6 +142,23 @@ def test_generators_invariants_and_determinism():
     assert gc0.size == 2 * ((29 * 20) + (30 * 19))
 
 
+@pytest.mark.parametrize("kind", ["rmat", "rmat_ef8", "uniform", "grid", "grid_noshort", "grid_thin"])
+def test_host_generator_matches_numpy(kind):
+    """The multi-threaded host generator (the reference arm's graph source)
+    builds the numpy restatement's graphs bit for bit."""
+    h = O.HostGen(threads=3)
+    a, b = {
+        "rmat": (lambda: h.rmat(13, 16, seed=5), lambda: gg.rmat(13, 16, seed=5)),
+        "rmat_ef8": (lambda: h.rmat(11, 8, seed=1), lambda: gg.rmat(11, 8, seed=1)),
+        "uniform": (lambda: h.uniform(3001, 32, seed=7), lambda: gg.uniform(3001, 32, seed=7)),
+        "grid": (lambda: h.grid(41, 29, 1, seed=2), lambda: gg.grid(41, 29, 1, seed=2)),
+        "grid_noshort": (lambda: h.grid(16, 16, 0, seed=2), lambda: gg.grid(16, 16, 0, seed=2)),
+        "grid_thin": (lambda: h.grid(2, 300, 5, seed=9), lambda: gg.grid(2, 300, 5, seed=9)),
+    }[kind]
+    (ho, hc), (no, nc) = a(), b()
+    assert np.array_equal(ho, no) and np.array_equal(hc, nc)
+
+
 def test_roots_are_seeded_and_have_out_edges():
     off, cols = gg.rmat(12, 16, seed=7)
     a = gg.roots(off, 64, seed=27491095)
