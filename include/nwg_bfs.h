@@ -87,7 +87,10 @@ int nwg_last_error(char* buf, size_t len);
  * std::get<0>(out_graph.to_be_indexed_) (containers/compressed.hpp:67-68,
  * algorithms/bfs.hpp:168) and in_graph[u] (bfs.hpp:216).  Host arrays are
  * uploaded once (the only bulk host-to-device copy); with NWG_REG_DEVICE
- * they are borrowed in place.  in_off/in_col NULL = symmetric graph. */
+ * they are borrowed in place.  in_off/in_col NULL = symmetric graph.
+ * NWG_REG_VALIDATE (host arrays) checks monotone offsets, column ids < n
+ * and, for a directed pair, that the in-CSR is the transpose of the
+ * out-CSR; without it the caller guarantees all three. */
 int nwg_graph_register(const uint64_t* out_off, const uint32_t* out_col, uint64_t n, const uint64_t* in_off,
                        const uint32_t* in_col, uint32_t flags, nwg_graph* out);
 
@@ -163,7 +166,11 @@ int nwg_graph_copy_csr(nwg_graph g, uint64_t* out_off, uint32_t* out_col, uint64
  * uint8: depth of vertex v from root i at depths_dev[i * n + v], 255 =
  * unreached; NWG_EOVERFLOW if some depth would be >= 255.  Runs on `stream`
  * (NULL = the workspace's own stream) and returns when done.  A workspace
- * holds about 388 * n bytes of device state (three bitsets and eight level
+ * The passes rely on the in-CSR being the exact transpose of the out-CSR
+ * (see nwg_graph_register): a pull reads the frontier words of in-
+ * neighbours, and a sparse push level leaves the frontier word of a vertex
+ * without out-edges unrefreshed, which a true transpose never lists as an
+ * in-neighbour.  A workspace holds about 388 * n bytes of device state (three bitsets and eight level
  * bit-planes of four 64-bit words per vertex, a touched-vertex list and its
  * bitmap) plus two frontier lists of 8 * (n + m / 256 + 1) bytes: about
  * 1.7 GB for RMAT-22, 6.8 GB for RMAT-24.
@@ -286,10 +293,13 @@ int nwg_server_run_trace(nwg_server s, uint32_t count, const uint32_t* graph, co
  * static device array of fixed size: n <= 2^20 and m <= 2^24 (larger graphs
  * return NWG_EINVAL before any launch).  Calls share that array: calls whose
  * GPU work overlaps race, so serialise them.  The first call on a device
- * looks the array's address up; make it before any stream capture.  The
- * level loop is driven from the host (a small read-back per step) on
- * `stream` (a cudaStream_t, NULL = legacy default stream); the call returns
- * when the traversal is complete. */
+ * looks the array's device address up and keeps it for the life of the
+ * process: do not use this entry point on a device across cudaDeviceReset,
+ * which unloads the module that holds the array.  The level loop is driven
+ * from the host (a small read-back per step) on `stream` (a cudaStream_t,
+ * NULL = legacy default stream) and the call synchronises that stream, so
+ * it must not be called while the stream is being captured into a CUDA
+ * graph; it returns when the traversal is complete. */
 int nwg_bfs_noalloc(const uint64_t* out_off, const uint32_t* out_col, const uint64_t* in_off, const uint32_t* in_col,
                     uint64_t n, uint32_t root, int alpha, int beta, uint32_t* parents_dev, void* stream);
 

@@ -42,6 +42,38 @@ int validate_csr(const uint64_t* off, const uint32_t* col, uint64_t n, const cha
   return NWG_OK;
 }
 
+// The in-CSR must be the transpose of the out-CSR (the contract of the
+// reference's bfs(out_graph, in_graph, ...)): for every v, in[v] holds, as a
+// multiset, exactly the u with v in out[u].  Checked by a counting sort of
+// the out-edges by target and a row-by-row comparison of sorted rows; O(n + m)
+// host memory.  Both CSRs have passed validate_csr.
+template <typename OffT>
+int validate_transpose(const OffT* out_off, const uint32_t* out_col, const OffT* in_off, const uint32_t* in_col,
+                       uint64_t n) {
+  const uint64_t        m = out_off[n];
+  std::vector<uint64_t> start(n + 1, 0);
+  for (uint64_t e = 0; e < m; ++e) start[out_col[e] + 1]++;
+  for (uint64_t v = 0; v < n; ++v) start[v + 1] += start[v];
+  for (uint64_t v = 0; v < n; ++v)
+    if (start[v + 1] - start[v] != (uint64_t)(in_off[v + 1] - in_off[v]))
+      return set_error(NWG_EINVAL, "in-graph is not the transpose of the out-graph: vertex " + std::to_string(v) +
+                                       " has " + std::to_string(in_off[v + 1] - in_off[v]) + " in-edges listed, " +
+                                       std::to_string(start[v + 1] - start[v]) + " out-edges pointing to it");
+  std::vector<uint32_t> t(m);
+  std::vector<uint64_t> pos(start.begin(), start.end() - 1);
+  for (uint64_t u = 0; u < n; ++u)
+    for (uint64_t e = out_off[u]; e < (uint64_t)out_off[u + 1]; ++e) t[pos[out_col[e]]++] = (uint32_t)u;
+  std::vector<uint32_t> row;
+  for (uint64_t v = 0; v < n; ++v) {  // t's rows are sorted already (sources visited in order)
+    row.assign(in_col + in_off[v], in_col + in_off[v + 1]);
+    std::sort(row.begin(), row.end());
+    if (!std::equal(row.begin(), row.end(), t.begin() + start[v]))
+      return set_error(NWG_EINVAL, "in-graph is not the transpose of the out-graph: in-edges of vertex " +
+                                       std::to_string(v) + " differ");
+  }
+  return NWG_OK;
+}
+
 int validate_csr32(const uint32_t* off, const uint32_t* col, uint64_t n, const char* which) {
   if (off[0] != 0) return set_error(NWG_EINVAL, std::string(which) + ": offsets[0] != 0");
   for (uint64_t i = 0; i < n; ++i)
@@ -131,6 +163,7 @@ int register_impl(const OffT* out_off, const uint32_t* out_col, uint64_t n, cons
       if (!g->symmetric) {
         rc = sizeof(OffT) == 8 ? validate_csr((const uint64_t*)in_off, in_col, n, "in-graph")
                                : validate_csr32((const uint32_t*)in_off, in_col, n, "in-graph");
+        if (!rc) rc = validate_transpose(out_off, out_col, in_off, in_col, n);
         if (rc) return fail(rc);
       }
     }

@@ -18,10 +18,13 @@
 // anything is launched.  Every call shares the one array, so calls whose
 // GPU work overlaps (two host threads, or two streams) race and corrupt each
 // other; serialise them.  The first call on a device looks the array's
-// device address up once (cudaGetSymbolAddress), so make that first call
-// before any stream capture on that device.  The level loop is driven from
-// the host (one small device-to-host read per step), so it is slower than
-// the CUDA-graph path of nwg_bfs.
+// device address up (cudaGetSymbolAddress) and keeps it for the life of the
+// process, so the entry point must not be used on a device across
+// cudaDeviceReset (which unloads the module holding the array).  The level
+// loop is driven from the host (one small device-to-host read per step,
+// which synchronises the caller's stream), so a call must not be made while
+// that stream is being captured into a CUDA graph, and it is slower than the
+// CUDA-graph path of nwg_bfs.
 #include <algorithm>
 #include <mutex>
 
@@ -125,6 +128,8 @@ extern "C" __attribute__((visibility("default"))) int nwg_bfs_noalloc(const uint
     P.qc[1]         = qc + kNaQcCap;
     P.qs_cap        = kNaQsCap;
     P.qc_cap        = kNaQcCap;
+    // Chunked vertices from out-degree 32 on (registered graphs use 64):
+    // kNaQcCap bounds the chunk entries for that threshold, m / 256 + min(n, m / 32) + 1.
     P.th            = Thresholds{32, 256, 8};
     P.ctrl          = reinterpret_cast<Ctrl*>(base + kNaOffCtrl);
     P.set_cond      = 0;

@@ -151,6 +151,14 @@ def test_edge_cases(nwg, port):
     assert e.value.code == nwg.NWG_EINVAL
     with pytest.raises(nwg.NwgError):
         nwg.Graph.from_csr(np.array([0, 2, 1], np.uint64), np.array([1, 0], np.uint32), validate=True)
+    # an in-CSR with the out-CSR's entry count that is not its transpose:
+    # out-edges 0 -> 1, 1 -> 0; the in-CSR claims 2 -> 0, and vertex 2 has no out-edges
+    off3, cols3 = np.array([0, 1, 2, 2], np.uint64), np.array([1, 0], np.uint32)
+    with pytest.raises(nwg.NwgError) as e:
+        nwg.Graph.from_csr(off3, cols3, np.array([0, 1, 2, 2], np.uint64), np.array([2, 0], np.uint32), validate=True)
+    assert e.value.code == nwg.NWG_EINVAL and "transpose" in str(e.value)
+    g = nwg.Graph.from_csr(off3, cols3, np.array([0, 1, 2, 2], np.uint64), np.array([1, 0], np.uint32), validate=True)
+    g.release()
 
 
 def test_device_generators_match_numpy(nwg):

@@ -72,3 +72,50 @@ def test_noalloc_rejects_graphs_over_the_limit(nwg):
         nwg.bfs_noalloc(off, col, n, 0, par)
     assert e.value.code == nwg.NWG_EINVAL
     assert "limit" in str(e.value)
+
+
+def test_noalloc_rejects_entry_counts_over_the_limit_and_non_transposes(nwg):
+    """Refusals that come before any launch: more CSR entries than the static
+    scratch holds (read from out_off[n]), and an in-CSR whose entry count
+    differs from the out-CSR's."""
+    import torch
+
+    big = (1 << 24) + 1
+    off = torch.tensor([0, big, big], dtype=torch.int64, device="cuda")
+    col = torch.zeros(4, dtype=torch.int32, device="cuda")
+    par = torch.empty(2, dtype=torch.int32, device="cuda")
+    with pytest.raises(nwg.NwgError) as e:
+        nwg.bfs_noalloc(off, col, 2, 0, par)
+    assert e.value.code == nwg.NWG_EINVAL and "limit" in str(e.value)
+    off = torch.tensor([0, 1, 2], dtype=torch.int64, device="cuda")
+    col = torch.tensor([1, 0, 0, 0], dtype=torch.int32, device="cuda")
+    in_off = torch.tensor([0, 1, 3], dtype=torch.int64, device="cuda")
+    in_col = torch.tensor([1, 0, 0, 0], dtype=torch.int32, device="cuda")
+    with pytest.raises(nwg.NwgError) as e:
+        nwg.bfs_noalloc(off, col, 2, 0, par, in_off, in_col)
+    assert e.value.code == nwg.NWG_EINVAL and "transpose" in str(e.value)
+
+
+@pytest.mark.parametrize("kind", ["uniform_at_n_limit", "rmat19"])
+def test_noalloc_near_the_limits(nwg, port, kind):
+    """Graphs at the static limits (2^20 vertices; just under 2^24 entries),
+    where the frontier queues fill to their full sizes: depths equal the
+    registered entry point's on two calls in a row."""
+    import torch
+
+    off, cols = gg.uniform(1 << 20, 15, seed=4) if kind == "uniform_at_n_limit" else gg.rmat(19, 16, seed=2)
+    n = off.size - 1
+    assert cols.size < (1 << 24)
+    g = nwg.Graph.from_csr(off, cols)
+    off_d, col_d = _dev(torch, off), _dev(torch, cols)
+    par_d = torch.empty(n, dtype=torch.int32, device="cuda")
+    for r in gg.roots(off, 2, seed=8):
+        r = int(r)
+        want = nwg.depths_from_parents(nwg.bfs(g, g, r), r)
+        for _ in range(2):
+            nwg.bfs_noalloc(off_d, col_d, n, r, par_d)
+            torch.cuda.synchronize()
+            got = par_d.cpu().numpy().view(np.uint32)
+            assert np.array_equal(nwg.depths_from_parents(got, r), want)
+            assert port.verify(off, cols, r, got)
+    g.release()
