@@ -560,6 +560,7 @@ __device__ __forceinline__ void init_step(const DobfsParams& p, uint32_t root, u
     c.b2q_steps = 0;
     c.status      = 0;
     c.pre_decided = 0;
+    c.bu_push     = 0;
     p.ctrl->bar.count = 0;
     p.ctrl->err       = 0;
     p.ctrl->decides   = 0;
@@ -589,6 +590,44 @@ __device__ __forceinline__ void trace_add(Ctrl* ctrl, CtrlHdr& c, uint8_t dir, u
     ctrl->trace_end_ns[c.trace_len]   = now - c.t_start;
     c.trace_len++;
   }
+}
+
+// Sets up a step of the top-down kernels over the queue in buffer c.cur
+// (writing buffer c.cur ^ 1) and returns the kernel that runs it: one
+// cluster for a tiny frontier, the persistent small grid for a small one,
+// the full grid otherwise.
+__device__ __forceinline__ uint32_t td_kernel_setup(CtrlHdr& c) {
+  const uint32_t nxt = c.cur ^ 1u;
+  c.qpos[nxt]        = 0;
+  c.qbig[nxt]        = 0;
+  c.nhub[nxt]        = 0;
+  c.acc_scout        = 0;
+  // warp work units of the step: chunk entries + groups of 32 small vertices
+  const uint64_t units = (c.qpos[c.cur] >> 32) + ((c.qpos[c.cur] & 0xFFFFFFFFull) + 31) / 32;
+  return units <= (uint64_t)kClusterUnits            ? kActTDCluster
+         : units <= (uint64_t)kSmallBlocks * kWarps ? kActTDSmall
+                                                    : kActTD;
+}
+
+// A bottom-up pull whose front is held as a queue (the first pull of a
+// phase: the frontier queue; or the pull after one run this way: its
+// discoveries) may run as a push from that queue with the top-down kernels.
+// On a symmetric graph the unvisited vertices with an in-neighbour in the
+// front are exactly the unvisited out-neighbours of the front, so the step
+// discovers the same set and the same awake count as bfs.hpp:211-228; only
+// a parent may name another front vertex, which BFSVerifier's rules allow.
+// The push is taken when its estimated bytes are below the pull's: a pull
+// reads about 48 B per candidate (unvisited, with in-edges: offsets and the
+// first column sector); a push reads an offset sector per front vertex,
+// 4 B per front out-edge and about 50 B per discovery (degree, claim,
+// parent, queue entry), discoveries estimated as at most twice the front.
+__device__ __forceinline__ bool pull_as_push(const DobfsParams& p, const CtrlHdr& c, uint64_t front,
+                                             uint64_t front_edges) {
+  if (!p.symmetric) return false;
+  const uint64_t excl = p.nzero + c.reached;
+  const uint64_t cand = p.n > excl ? p.n - excl : 0;
+  const uint64_t wins = min(cand, 2 * front);
+  return 32 * front + 4 * front_edges + 50 * wins < 48 * cand;
 }
 
 // ---------------------------------------------------------------------------
@@ -621,6 +660,37 @@ __device__ uint32_t decide_core(const DobfsParams& p) {
     case kActTDCluster: {
       const uint32_t nxt = c.cur ^ 1u;
       const uint64_t nq  = frontier_size(c, nxt);
+      if (c.bu_push) {  // a bottom-up pull run as a push: the pull's bookkeeping
+        const uint64_t awake = nq;
+        trace_add(p.ctrl, c, 1, c.old_awake, awake, now);
+        c.bu_steps++;
+        c.reached += awake;
+        c.cur = nxt;  // the discoveries, held as a queue, are the next front
+        if (awake > 0) c.levels++;
+        if (awake >= c.old_awake || awake > N / c.beta) {  // bfs.hpp:229
+          c.old_awake   = awake;                           // bfs.hpp:206
+          c.awake_count = awake;
+          if (pull_as_push(p, c, awake, c.acc_scout)) {
+            next = td_kernel_setup(c);
+          } else {  // a pull over V, which holds every visited vertex
+            c.bu_push   = 0;
+            c.acc_awake = 0;
+            c.bu_mode   = 0;
+            c.bm        = 1;
+            next        = kActBU;
+          }
+        } else if (awake == 0) {
+          done = true;  // bfs.hpp:231-233
+        } else {
+          // the phase ends; the discoveries are already the queue that
+          // bitmap->queue would build (bfs.hpp:235-239)
+          c.bu_push      = 0;
+          c.awake_count  = awake;
+          c.scout_count  = 1;  // bfs.hpp:241
+          queue_decision = true;
+        }
+        break;
+      }
       trace_add(p.ctrl, c, 0, frontier_size(c, c.cur), nq, now);
       c.td_steps++;
       c.reached += nq;
@@ -673,22 +743,18 @@ __device__ uint32_t decide_core(const DobfsParams& p) {
     if (!c.topdown_only && c.scout_count > c.edges_to_check / c.alpha) {  // bfs.hpp:186
       c.awake_count = nq;                                                // bfs.hpp:199-202
       c.old_awake   = nq;
-      c.acc_awake   = 0;
-      c.bu_mode     = 0;
-      c.bm          = 1;  // the first pull writes C0
-        next          = kActBU;
+      if (pull_as_push(p, c, nq, c.scout_count)) {  // scout_count: the frontier's out-edges
+        c.bu_push = 1;
+        next      = td_kernel_setup(c);
+      } else {
+        c.acc_awake = 0;
+        c.bu_mode   = 0;
+        c.bm        = 1;  // the first pull writes C0
+        next        = kActBU;
+      }
     } else {
       c.edges_to_check -= c.scout_count;  // bfs.hpp:244
-      const uint32_t nxt = c.cur ^ 1u;
-      c.qpos[nxt] = 0;
-      c.qbig[nxt] = 0;
-      c.nhub[nxt] = 0;
-      c.acc_scout = 0;
-      // warp work units of the step: chunk entries + groups of 32 small vertices
-      const uint64_t units = (c.qpos[c.cur] >> 32) + ((c.qpos[c.cur] & 0xFFFFFFFFull) + 31) / 32;
-      next                 = units <= (uint64_t)kClusterUnits            ? kActTDCluster
-                             : units <= (uint64_t)kSmallBlocks * kWarps ? kActTDSmall
-                                                                        : kActTD;
+      next = td_kernel_setup(c);
     }
   }
   if (!done && ++c.steps > c.max_steps) {
@@ -954,16 +1020,23 @@ __device__ __forceinline__ uint32_t compact_tile(uint32_t bits, uint16_t* list) 
 //
 // Warps take tiles of kBuTileWords bitmap words (256 vertices), interleaved
 // over the grid (about seven tiles per warp at 2^24 vertices, so uneven tiles
-// average out).  A lane reads one word of
-// V, of the previous pull's C and of Z, folds C into V (the owner is the only
-// writer), and the tile's candidates (unvisited, with in-edges) are compacted
-// into a per-warp list in shared memory.  The
-// warp then takes 32 candidates at a time, one per lane, so 32 independent
-// in-edge scans are in flight per warp regardless of how sparse the
-// candidates are.  A lane scans its first kBuLane in-neighbours alone,
-// kBuProbe per round with independent loads; lanes still unresolved with
-// edges left are scanned by the whole warp, 32 in-edges per step.  The first hit in row order becomes the parent, exactly as the
-// reference's sequential scan with `break`.
+// average out).  A lane reads one word of V, of the previous pull's C and of
+// Z, folds C into V (the owner is the only writer), and the tile's
+// candidates (unvisited, with in-edges) are compacted into a per-warp list
+// in shared memory.
+//
+// The candidates then stream through the lanes.  Each lane holds the
+// candidate whose in-edges it is testing and the next one, whose in-CSR
+// offsets are already loading.  When a lane's scan ends (a hit, or its list
+// is exhausted) it promotes its next candidate, and the lanes that need a
+// next one take the following list entries with one ballot.  A round tests
+// kBuProbe in-edges of the current candidate with independent loads.  Every
+// lane thus keeps a scan in flight until the tile's list runs out (a batch
+// of 32 candidates no longer waits for its longest scan), and the offsets'
+// latency hides behind the current scan.  A lane that has tested kBuLane
+// in-edges without a hit hands the rest of its list to the whole warp, 32
+// in-edges per step.  The first hit in row order becomes the parent, exactly
+// as the reference's sequential scan with `break`.
 __device__ __forceinline__ void bu_step(const DobfsParams& p, uint32_t block, uint32_t nblocks) {
   __shared__ uint16_t s_cand[kWarps][kBuTileWords * 32];
   __shared__ uint32_t s_new[kWarps][kBuTileWords];
@@ -979,6 +1052,7 @@ __device__ __forceinline__ void bu_step(const DobfsParams& p, uint32_t block, ui
   uint16_t* const cand    = s_cand[wib];
   uint32_t* const fresh   = s_new[wib];
   const uint64_t  ntiles  = (p.nwords + kBuTileWords - 1) / kBuTileWords;
+  const unsigned  lt_mask = (1u << lane) - 1u;
   uint32_t        awake   = 0;
 
   const uint64_t  gwarp   = (uint64_t)block * kWarps + wib;
@@ -995,49 +1069,63 @@ __device__ __forceinline__ void bu_step(const DobfsParams& p, uint32_t block, ui
     }
     if (lane < kBuTileWords) fresh[lane] = 0;
     const uint32_t total = compact_tile(cm, cand);
-
     const uint64_t vbase = t * kBuTileWords * 32;
-    for (uint32_t j = 0; j < total; j += 32) {
-      const bool     mine = j + lane < total;
-      const uint32_t loc  = mine ? cand[j + lane] : 0u;
-      const uint64_t u    = vbase + loc;
-      uint64_t       beg = 0, end = 0;
-      if (mine) {
-        beg = p.in_off[u];
-        end = p.in_off[u + 1];
-      }
-      bool           found = false;
-      uint32_t       par   = 0;
-      uint64_t       e     = beg;
-      const uint64_t lim   = min(end, beg + kBuLane);
-      // each lane scans its own first kBuLane in-edges, kBuProbe per round
-      // (independent column and bitmap loads), until a hit
-      while (__any_sync(kFullMask, mine && !found && e < lim)) {
-        if (mine && !found && e < lim) {
-          uint32_t nb[kBuProbe];
+
+    // current candidate (cu: local index, ce: next in-edge, cend, cn: edges
+    // tested) and next candidate (nu, nb, nend, offsets in flight)
+    uint32_t cu = 0, nu = 0, cn = 0;
+    uint64_t ce = 0, cend = 0, nb = 0, nend = 0;
+    bool     cv = false, nv = false;
+    if (lane < total) {
+      cu   = cand[lane];
+      ce   = p.in_off[vbase + cu];
+      cend = p.in_off[vbase + cu + 1];
+      cv   = true;
+    }
+    uint32_t ptr = min(total, 32u);  // next unassigned list entry (warp-uniform)
+    if (ptr + lane < total) {
+      nu   = cand[ptr + lane];
+      nb   = p.in_off[vbase + nu];
+      nend = p.in_off[vbase + nu + 1];
+      nv   = true;
+    }
+    ptr = min(total, ptr + 32u);
+
+    while (__any_sync(kFullMask, cv)) {
+      bool     found = false, handoff = false;
+      uint32_t par   = 0;
+      if (cv) {
+        uint32_t nbv[kBuProbe];
 #pragma unroll
-          for (int k = 0; k < kBuProbe; ++k) nb[k] = (e + k < lim) ? __ldg(p.in_col + e + k) : kNull;
-          uint32_t hit = 0;
+        for (int k = 0; k < kBuProbe; ++k) nbv[k] = (ce + k < cend) ? __ldg(p.in_col + ce + k) : kNull;
+        uint32_t hit = 0;
 #pragma unroll
-          for (int k = 0; k < kBuProbe; ++k)
-            if (nb[k] != kNull && ((__ldg(front + (nb[k] >> 5)) >> (nb[k] & 31)) & 1u)) hit |= 1u << k;
-          if (hit) {
-            const int k = __ffs(hit) - 1;
+        for (int k = 0; k < kBuProbe; ++k)
+          if (nbv[k] != kNull && ((__ldg(front + (nbv[k] >> 5)) >> (nbv[k] & 31)) & 1u)) hit |= 1u << k;
+        if (hit) {
+          const int k = __ffs(hit) - 1;
 #pragma unroll
-            for (int q = 0; q < kBuProbe; ++q)
-              if (q == k) par = nb[q];
-            found = true;
+          for (int q = 0; q < kBuProbe; ++q)
+            if (q == k) par = nbv[q];
+          found = true;
+        } else {
+          ce += kBuProbe;
+          cn += kBuProbe;
+          if (ce >= cend) {
+            cv = false;  // list exhausted: no parent this pull
+          } else if (cn >= kBuLane) {
+            handoff = true;  // long list: the warp scans the rest
           }
-          e = min(lim, e + kBuProbe);
         }
       }
-      const uint64_t rest = e;  // long lists: the whole warp scans the rest
-      unsigned       pend = __ballot_sync(kFullMask, mine && !found && rest < end);
+      unsigned pend = __ballot_sync(kFullMask, handoff);
       while (pend) {
         const int leader = __ffs(pend) - 1;
         pend &= pend - 1;
-        const uint64_t b  = __shfl_sync(kFullMask, rest, leader);
-        const uint64_t en = __shfl_sync(kFullMask, end, leader);
+        const uint64_t b  = __shfl_sync(kFullMask, ce, leader);
+        const uint64_t en = __shfl_sync(kFullMask, cend, leader);
+        bool           lf = false;
+        uint32_t       lp = 0;
         for (uint64_t base = b; base < en; base += 32) {
           const uint64_t i = base + lane;
           uint32_t       v = 0;
@@ -1048,18 +1136,40 @@ __device__ __forceinline__ void bu_step(const DobfsParams& p, uint32_t block, ui
           }
           const unsigned hm = __ballot_sync(kFullMask, h);
           if (hm) {
-            const uint32_t pv = __shfl_sync(kFullMask, v, __ffs(hm) - 1);
-            if ((int)lane == leader) {
-              found = true;
-              par   = pv;
-            }
+            lp = __shfl_sync(kFullMask, v, __ffs(hm) - 1);
+            lf = true;
             break;
           }
         }
+        if ((int)lane == leader) {
+          found = lf;
+          par   = lp;
+          cv    = false;
+        }
       }
       if (found) {
-        parents[u] = par;
-        atomicOr(&fresh[loc >> 5], 1u << (loc & 31));
+        parents[vbase + cu] = par;
+        atomicOr(&fresh[cu >> 5], 1u << (cu & 31));
+        cv = false;
+      }
+      if (!cv && nv) {  // promote the next candidate
+        cu   = nu;
+        ce   = nb;
+        cend = nend;
+        cn   = 0;
+        cv   = true;
+        nv   = false;
+      }
+      if (ptr < total) {  // warp-uniform: hand the next entries to the lanes without a next candidate
+        const unsigned need = __ballot_sync(kFullMask, !nv);
+        const uint32_t rank = __popc(need & lt_mask);
+        if (!nv && ptr + rank < total) {
+          nu   = cand[ptr + rank];
+          nb   = p.in_off[vbase + nu];
+          nend = p.in_off[vbase + nu + 1];
+          nv   = true;
+        }
+        ptr = min(total, ptr + (uint32_t)__popc(need));
       }
     }
     __syncwarp();
@@ -1131,6 +1241,14 @@ __global__ void k_zero_indegree(const uint64_t* __restrict__ in_off, uint64_t n,
     const unsigned b    = __ballot_sync(kFullMask, zero);
     if (lane == 0) Z[w] = b;
   }
+}
+
+__global__ void k_popc_words(const uint32_t* __restrict__ w, uint64_t nwords, unsigned long long* out) {
+  unsigned long long c = 0;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nwords; i += (uint64_t)gridDim.x * blockDim.x)
+    c += __popc(w[i]);
+  c = block_sum(c);
+  if (threadIdx.x == 0 && c) atomicAdd(out, c);
 }
 
 __global__ void k_component(const uint64_t* __restrict__ off, const uint32_t* __restrict__ parents, uint64_t n,
@@ -1220,6 +1338,8 @@ __global__ void __launch_bounds__(kThreads) k_ragged(RaggedParams rp) {
     p.qs_cap               = L.qs_cap;
     p.qc_cap               = L.qc_cap;
     p.th                   = Thresholds{item.warp_min, 256, 8};
+    p.nzero                = 0;  // unknown here: the push-or-pull estimate then counts isolated vertices too
+    p.symmetric            = 1;  // packed graphs are symmetric
     p.ctrl                 = reinterpret_cast<Ctrl*>(slot + L.ctrl);
     p.set_cond             = 0;
     init_step(p, item.root, (uint32_t)item.alpha, (uint32_t)item.beta, rp.parents + item.out_base, 0u, 0, 1);
@@ -1416,6 +1536,8 @@ int ws_init(GraphDev* g, Workspace* ws) {
   P.hubrec[1]    = ws->hubbuf + hub_cap;
   P.hub_cap      = hub_cap;
   P.th           = g->th;
+  P.nzero        = g->nzero;
+  P.symmetric    = g->symmetric ? 1u : 0u;
   P.ctrl         = ws->ctrl;
   return build_exec(ws);
 }
@@ -1538,12 +1660,29 @@ void fill_stats(const Ctrl& c, nwg_bfs_stats* s) {
   s->first_decide_ns = c.t_first_decide;
 }
 
+// Builds the in-degree-zero bitmap Z and counts the vertices without
+// in-edges (g->nzero; the bits past n are set in Z and not counted).
+// Synchronises the stream.
 int build_zero_indegree(GraphDev* g, cudaStream_t stream) {
   const uint32_t nwords = (uint32_t)((g->n + 31) / 32);
   NWG_CUDA_TRY(cudaMalloc(&g->Z, std::max<uint32_t>(nwords, 1) * sizeof(uint32_t)));
+  g->nzero = 0;
   if (nwords) {
     k_zero_indegree<<<grid_for(g, 4), kThreads, 0, stream>>>(g->in_off, g->n, nwords, g->Z);
     NWG_CUDA_TRY(cudaGetLastError());
+    unsigned long long* d = nullptr;
+    NWG_CUDA_TRY(cudaMalloc(&d, sizeof(unsigned long long)));
+    unsigned long long h  = 0;
+    cudaError_t        e  = cudaMemsetAsync(d, 0, sizeof(h), stream);
+    if (e == cudaSuccess) {
+      k_popc_words<<<grid_for(g, 4), kThreads, 0, stream>>>(g->Z, nwords, d);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    cudaFree(d);
+    if (e != cudaSuccess) return cuda_error(e, "zero in-degree count");
+    g->nzero = h - ((uint64_t)nwords * 32 - g->n);
   }
   return NWG_OK;
 }

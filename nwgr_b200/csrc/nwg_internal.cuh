@@ -73,6 +73,7 @@ struct alignas(16) CtrlHdr {
   uint32_t steps, levels, td_steps, bu_steps, b2q_steps;
   int32_t  status;
   uint32_t pre_decided;  // the previous action kernel already made the next decision
+  uint32_t bu_push;      // the top-down kernel's current step is a bottom-up pull run as a push
   unsigned long long reached;
   unsigned long long t_start;  // %globaltimer at init (ns)
   uint32_t trace_len;
@@ -126,6 +127,8 @@ struct DobfsParams {
   HubRec*         hubrec[2];  // [buffer] deferred hub records (null: hubs are written by their warp)
   uint64_t        hub_cap;
   Thresholds      th;
+  uint64_t        nzero;      // vertices without in-edges (0 where unknown: only a cost estimate uses it)
+  uint32_t        symmetric;  // the in-CSR is the out-CSR (a pull may then run as a push)
   Ctrl*           ctrl;
   cudaGraphConditionalHandle h_loop;
   cudaGraphConditionalHandle h_switch;
@@ -252,6 +255,7 @@ struct GraphDev {
   uint64_t* in_off = nullptr;
   uint32_t* in_col = nullptr;
   uint32_t* Z = nullptr;  // in-degree-zero bitmap
+  uint64_t  nzero = 0;    // its population (vertices without in-edges)
   bool      owns_out = false, owns_in = false, symmetric = true;
   int       sm_count = 148;
   // out-degree >= 64 goes to the chunk queue: 2.0% (RMAT-24) and 2.4%

@@ -131,6 +131,8 @@ extern "C" __attribute__((visibility("default"))) int nwg_bfs_noalloc(const uint
     // Chunked vertices from out-degree 32 on (registered graphs use 64):
     // kNaQcCap bounds the chunk entries for that threshold, m / 256 + min(n, m / 32) + 1.
     P.th            = Thresholds{32, 256, 8};
+    P.symmetric     = in_off ? 0u : 1u;
+    P.nzero         = 0;  // not counted here (it would need a reduction and a read-back)
     P.ctrl          = reinterpret_cast<Ctrl*>(base + kNaOffCtrl);
     P.set_cond      = 0;
 
