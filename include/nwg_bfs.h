@@ -164,7 +164,14 @@ int nwg_graph_copy_csr(nwg_graph g, uint64_t* out_off, uint32_t* out_col, uint64
  * unexplored edges / alpha (4 suits it better than the single-source 15: a
  * multi-source pull rarely stops early).  depths_dev is a device array [k][n] of
  * uint8: depth of vertex v from root i at depths_dev[i * n + v], 255 =
- * unreached; NWG_EOVERFLOW if some depth would be >= 255.  Runs on `stream`
+ * unreached.  A source whose depths reach 255 (a graph whose diameter passes
+ * 254) does not spoil the others: every other row is exact, that source's
+ * row holds its depths up to 254 (255 beyond), and the call returns
+ * NWG_EOVERFLOW (stats->deep_sources counts such sources; nwg_msbfs_ex
+ * flags them one by one and answers them exactly in uint16).  Calls of more
+ * than 256 sources keep up to four passes in flight, each on its own copy of
+ * the pass state and its own stream (the extra copies are made on the first
+ * such call and kept with the workspace).  Runs on `stream`
  * (NULL = the workspace's own stream) and returns when done.  A workspace
  * The passes rely on the in-CSR being the exact transpose of the out-CSR
  * (see nwg_graph_register): a pull reads the frontier words of in-
@@ -191,11 +198,23 @@ typedef struct {
   float trace_ms[NWG_MS_TRACE_CAP];
   uint64_t trace_frontier_edges[NWG_MS_TRACE_CAP];
   uint64_t trace_discovered[NWG_MS_TRACE_CAP];
+  uint32_t deep_sources; /* sources whose depths reach 255 or more */
 } nwg_msbfs_stats;
 int nwg_msbfs_ws_create(nwg_graph g, nwg_msbfs_ws* out);
 int nwg_msbfs_ws_destroy(nwg_msbfs_ws ws);
 int nwg_msbfs(nwg_msbfs_ws ws, const uint32_t* roots_host, uint32_t k, uint8_t* depths_dev, int alpha, void* stream,
               nwg_msbfs_stats* stats);
+/* nwg_msbfs with the row width chosen and deep sources reported per source
+ * (no reference counterpart either).  depth_bytes = 1: uint8 rows as
+ * nwg_msbfs writes them, but a deep source is not an error: the call returns
+ * NWG_OK and deep_flags_host[i] = 1 marks each row i that stops at 254.
+ * depth_bytes = 2: rows of uint16 (depths_dev[i * n + v], 0xFFFF =
+ * unreached), all exact: a deep source's row comes from one single-source
+ * traversal (nw::graph::bfs semantics, bfs.hpp:160-311) and its parents'
+ * depths, on a workspace made and freed for the call; NWG_EOVERFLOW only if
+ * a depth reaches 65535.  deep_flags_host (k bytes) may be NULL. */
+int nwg_msbfs_ex(nwg_msbfs_ws ws, const uint32_t* roots_host, uint32_t k, void* depths_dev, uint32_t depth_bytes,
+                 uint8_t* deep_flags_host, int alpha, void* stream, nwg_msbfs_stats* stats);
 
 /* Ragged batch: many small graphs packed in HBM once, and a table of
  * (graph, root) traversals run in ONE persistent launch (replayed as a CUDA
@@ -233,15 +252,20 @@ int nwg_ragged_bfs(nwg_ragged r, uint32_t num_items, const nwg_ragged_item* item
                    float* device_ms);
 
 /* Serving: (graph, root) queries against registered graphs kept resident in
- * HBM, answered as uint8 depth rows (depth per vertex, 255 = unreached; n
- * bytes of the query's graph).  No reference counterpart: NWGraph answers
+ * HBM, answered as depth rows: uint8 (depth per vertex, 255 = unreached; n
+ * bytes of the query's graph) or, with depth_bytes = 2, uint16 (0xFFFF =
+ * unreached; 2 n bytes).  A query whose depths reach 255 is answered
+ * exactly in uint16 rows; in uint8 rows that query alone fails with
+ * NWG_EOVERFLOW (its row then holds the depths up to 254, 255 beyond) and
+ * the others coalesced with it are answered as usual.  No reference counterpart: NWGraph answers
  * one bfs call at a time; each answer equals the depths of that single-source
  * BFS.  `slots` worker threads, each with its own CUDA stream and
  * multi-source workspace, run batches concurrently: a free slot takes the
  * graph of the oldest waiting query and coalesces up to max_batch waiting
  * queries on that graph into one multi-source pass (nwg_msbfs).  Admission:
- * a query taken by a slot holds 2.5 * n bytes of state (its device depth
- * row, its pinned host row and one bit per vertex in four bitsets) until its
+ * a query taken by a slot holds (2 * depth_bytes + 0.5) * n bytes of state
+ * (its device depth row, its pinned host row and one bit per vertex in four
+ * bitsets) until its
  * answer is in host memory; taken state never exceeds the budget left after
  * the slots' fixed buffers (max_batch 256 rows of the largest graph, device
  * and pinned, plus the workspace), and queries that do not fit wait.  All
@@ -252,6 +276,7 @@ typedef struct {
   uint32_t max_batch;    /* queries per multi-source pass (0 = 256, at most 256) */
   uint64_t budget_bytes; /* slots' buffers + per-query state, device and pinned host (0 = 16 GiB) */
   int32_t alpha;         /* push/pull switch of the multi-source pass (0 = 4) */
+  uint32_t depth_bytes;  /* answer row bytes per vertex: 1 (uint8) or 2 (uint16); 0 = 1 */
 } nwg_server_config;
 typedef struct {
   uint64_t queries, batches, failed;
@@ -268,8 +293,8 @@ typedef struct {
 int nwg_server_create(const nwg_graph* graphs, uint32_t num_graphs, const nwg_server_config* cfg, nwg_server* out);
 /* Stops the workers and frees the slots; no nwg_server_wait may be pending. */
 int nwg_server_destroy(nwg_server s);
-/* Queues one query; depths_host (n bytes of the graph, or NULL) receives the
- * answer.  nwg_server_wait blocks until that query is answered and returns
+/* Queues one query; depths_host (n * depth_bytes bytes of the graph, or
+ * NULL) receives the answer.  nwg_server_wait blocks until that query is answered and returns
  * its status; latency_us = submit to answer. */
 int nwg_server_submit(nwg_server s, uint32_t graph, uint32_t root, uint8_t* depths_host, uint64_t* ticket);
 int nwg_server_wait(nwg_server s, uint64_t ticket, double* latency_us);

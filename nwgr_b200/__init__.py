@@ -39,7 +39,7 @@ EXPORTED = (
     "nwg_graph_info", "nwg_bfs", "nwg_ws_create", "nwg_ws_destroy", "nwg_bfs_async", "nwg_ws_stats",
     "nwg_bfs_topdown", "nwg_bfs_stepped", "nwg_component_edges", "nwg_graph_copy_csr", "nwg_gen_rmat", "nwg_gen_uniform",
     "nwg_gen_grid", "nwg_pick_roots", "nwg_bfs_noalloc", "nwg_msbfs_ws_create", "nwg_msbfs_ws_destroy",
-    "nwg_msbfs", "nwg_ragged_register", "nwg_ragged_release", "nwg_ragged_info", "nwg_ragged_bfs",
+    "nwg_msbfs", "nwg_msbfs_ex", "nwg_ragged_register", "nwg_ragged_release", "nwg_ragged_info", "nwg_ragged_bfs",
     "nwg_server_create", "nwg_server_destroy", "nwg_server_submit", "nwg_server_wait", "nwg_server_run_trace",
     "nwg_verify", "nwg_graph_read", "nwg_graph_write_nwbin", "nwg_bc", "nwg_selftest_wait_timeout",
 )
@@ -89,7 +89,7 @@ class MsStats(C.Structure):
                 ("push_levels", C.c_uint32), ("pull_levels", C.c_uint32), ("device_ms", C.c_float),
                 ("trace_len", C.c_uint32), ("trace_pull", C.c_uint8 * MS_TRACE_CAP),
                 ("trace_ms", C.c_float * MS_TRACE_CAP), ("trace_frontier_edges", C.c_uint64 * MS_TRACE_CAP),
-                ("trace_discovered", C.c_uint64 * MS_TRACE_CAP)]
+                ("trace_discovered", C.c_uint64 * MS_TRACE_CAP), ("deep_sources", C.c_uint32)]
 
     def trace(self):
         k = self.trace_len
@@ -109,7 +109,8 @@ class RaggedResult(C.Structure):
 
 
 class ServerConfig(C.Structure):
-    _fields_ = [("slots", C.c_uint32), ("max_batch", C.c_uint32), ("budget_bytes", C.c_uint64), ("alpha", C.c_int32)]
+    _fields_ = [("slots", C.c_uint32), ("max_batch", C.c_uint32), ("budget_bytes", C.c_uint64), ("alpha", C.c_int32),
+                ("depth_bytes", C.c_uint32)]
 
 
 class ServerStats(C.Structure):
@@ -167,6 +168,7 @@ def _load():
         "nwg_msbfs_ws_create": (_int, [_vp, C.POINTER(_vp)]),
         "nwg_msbfs_ws_destroy": (_int, [_vp]),
         "nwg_msbfs": (_int, [_vp, _vp, _u32, _vp, _int, _vp, C.POINTER(MsStats)]),
+        "nwg_msbfs_ex": (_int, [_vp, _vp, _u32, _vp, _u32, _vp, _int, _vp, C.POINTER(MsStats)]),
         "nwg_ragged_register": (_int, [_u32, _vp, _vp, _vp, C.POINTER(_vp)]),
         "nwg_ragged_release": (_int, [_vp]),
         "nwg_ragged_info": (_int, [_vp, C.POINTER(_u32), C.POINTER(_u64), C.POINTER(_u64), C.POINTER(_u64)]),
@@ -343,21 +345,43 @@ class MsWorkspace:
         check(lib.nwg_msbfs(self.h, roots.ctypes.data, roots.size, _ptr(depths_dev), alpha, _ptr(stream), C.byref(st)))
         return st
 
+    def run_ex(self, roots, depths_dev, deep_flags=None, alpha: int = MS_ALPHA, stream=None) -> MsStats:
+        """nwg_msbfs_ex: depths_dev is a device [k][n] array of uint8 (255 =
+        unreached) or of 16-bit integers (read as uint16, 0xFFFF = unreached).
+        uint8 rows of sources whose depths reach 255 stop at 254 and are
+        flagged in deep_flags (host uint8 array of k, optional); uint16 rows
+        are exact for every source."""
+        roots = np.ascontiguousarray(roots, dtype=np.uint32)
+        width = depths_dev.element_size() if hasattr(depths_dev, "element_size") else depths_dev.dtype.itemsize
+        if deep_flags is not None:
+            assert deep_flags.dtype == np.uint8 and deep_flags.size >= roots.size and deep_flags.flags.c_contiguous
+        st = MsStats()
+        check(lib.nwg_msbfs_ex(self.h, roots.ctypes.data, roots.size, _ptr(depths_dev), int(width),
+                               None if deep_flags is None else deep_flags.ctypes.data, alpha, _ptr(stream),
+                               C.byref(st)))
+        return st
+
     def close(self):
         if self.h and self.g.h:
             check(lib.nwg_msbfs_ws_destroy(self.h))
         self.h = None
 
 
-def msbfs(g: Graph, roots, alpha: int = MS_ALPHA):
-    """Batched multi-source BFS; returns host uint8 depths [k][n] (255 =
-    unreached) and the MsStats.  Uses torch for the device output buffer."""
+def msbfs(g: Graph, roots, alpha: int = MS_ALPHA, depth_bytes: int = 1):
+    """Batched multi-source BFS; returns host depths [k][n] and the MsStats.
+    depth_bytes 1: uint8 (255 = unreached; raises NwgError NWG_EOVERFLOW if a
+    depth reaches 255); 2: uint16 (0xFFFF = unreached), exact for any
+    depth below 65535.  Uses torch for the device output buffer."""
     import torch
 
     roots = np.ascontiguousarray(roots, dtype=np.uint32)
-    out = torch.empty((roots.size, g.n), dtype=torch.uint8, device="cuda")
     ws = MsWorkspace(g)
     try:
+        if depth_bytes == 2:
+            out = torch.empty((roots.size, g.n), dtype=torch.int16, device="cuda")
+            st = ws.run_ex(roots, out, None, alpha)
+            return out.cpu().numpy().view(np.uint16), st
+        out = torch.empty((roots.size, g.n), dtype=torch.uint8, device="cuda")
         st = ws.run(roots, out, alpha)
     finally:
         ws.close()
@@ -413,22 +437,27 @@ class RaggedBatch:
 
 class Server:
     """Query server over resident graphs (nwg_server): (graph index, root)
-    queries answered as uint8 depth rows (255 = unreached), same-graph
-    queries coalesced into multi-source passes, `slots` batches in flight
-    at once, admission against `budget_bytes`."""
+    queries answered as depth rows -- uint8 (255 = unreached) or, with
+    depth_bytes=2, uint16 (0xFFFF = unreached) -- same-graph queries
+    coalesced into multi-source passes, `slots` batches in flight at once,
+    admission against `budget_bytes`."""
 
-    def __init__(self, graphs, slots: int = 16, max_batch: int = 256, budget_bytes: int = 16 << 30, alpha: int = 0):
+    def __init__(self, graphs, slots: int = 16, max_batch: int = 256, budget_bytes: int = 16 << 30, alpha: int = 0,
+                 depth_bytes: int = 1):
         self.graphs = list(graphs)  # kept alive: the server borrows them
+        self.depth_bytes = int(depth_bytes)
+        self.dtype = np.uint16 if self.depth_bytes == 2 else np.uint8
         hs = (_vp * len(self.graphs))(*[g.h for g in self.graphs])
-        cfg = ServerConfig(int(slots), int(max_batch), int(budget_bytes), int(alpha))
+        cfg = ServerConfig(int(slots), int(max_batch), int(budget_bytes), int(alpha), self.depth_bytes)
         h = _vp()
         check(lib.nwg_server_create(hs, len(self.graphs), C.byref(cfg), C.byref(h)))
         self.h = h.value
 
     def submit(self, graph: int, root: int, out: np.ndarray | None = None) -> int:
-        """Queues one query; `out` (uint8, n of the graph) receives the answer."""
+        """Queues one query; `out` (uint8, or uint16 with depth_bytes=2; n of
+        the graph) receives the answer."""
         if out is not None:
-            assert out.dtype == np.uint8 and out.flags.c_contiguous and out.size >= self.graphs[graph].n
+            assert out.dtype == self.dtype and out.flags.c_contiguous and out.size >= self.graphs[graph].n
         t = _u64()
         check(lib.nwg_server_submit(self.h, int(graph), int(root), None if out is None else out.ctypes.data,
                                     C.byref(t)))
@@ -442,8 +471,8 @@ class Server:
 
     def run_trace(self, graph_ids, roots, arrival_us, outputs=None):
         """Open-loop replay: query i released at arrival_us[i].  outputs: None
-        or a list of uint8 arrays (None entries allowed).  Returns (latency
-        ms per query, batch size per query, ServerStats)."""
+        or a list of arrays of the server's row type (None entries allowed).
+        Returns (latency ms per query, batch size per query, ServerStats)."""
         g = np.ascontiguousarray(graph_ids, np.uint32)
         r = np.ascontiguousarray(roots, np.uint32)
         a = np.ascontiguousarray(arrival_us, np.float64)
@@ -451,6 +480,8 @@ class Server:
         assert r.size == k and a.size == k
         outp = None
         if outputs is not None:
+            assert all(o is None or (o.dtype == self.dtype and o.size >= self.graphs[gi].n)
+                       for o, gi in zip(outputs, g.tolist()))
             outp = (C.c_void_p * k)(*[None if o is None else o.ctypes.data for o in outputs])
         lat = np.zeros(k, np.float64)
         bs = np.zeros(k, np.uint32)

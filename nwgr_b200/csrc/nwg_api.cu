@@ -484,22 +484,45 @@ NWG_API int nwg_msbfs_ws_destroy(nwg_msbfs_ws h) {
   NWG_GUARD_END
 }
 
-NWG_API int nwg_msbfs(nwg_msbfs_ws h, const uint32_t* roots_host, uint32_t k, uint8_t* depths_dev, int alpha,
-                      void* stream, nwg_msbfs_stats* stats) {
-  NWG_GUARD_BEGIN
+namespace {
+int msbfs_common(nwg_msbfs_ws h, const uint32_t* roots_host, uint32_t k, void* depths_dev, uint32_t depth_bytes,
+                 uint8_t* deep_flags, int alpha, void* stream, nwg_msbfs_stats* stats) {
   if (!h || (!roots_host && k) || (!depths_dev && k)) return set_error(NWG_EINVAL, "NULL argument");
   auto*           ws = reinterpret_cast<MsWorkspace*>(h);
   DeviceGuard     dg(ws->g->device);
   nwg_msbfs_stats st = {};
   cudaStream_t    s  = stream ? reinterpret_cast<cudaStream_t>(stream) : ws->stream;
   NWG_CUDA_TRY(cudaEventRecord(ws->ev0, s));
-  int rc = ms_run(ws, roots_host, k, depths_dev, alpha, s, &st);
+  int rc = ms_run(ws, roots_host, k, depths_dev, depth_bytes, deep_flags, alpha, s, &st);
   NWG_CUDA_TRY(cudaEventRecord(ws->ev1, s));
   NWG_CUDA_TRY(cudaEventSynchronize(ws->ev1));
   cudaEventElapsedTime(&st.device_ms, ws->ev0, ws->ev1);
   st.status = rc;
   if (stats) *stats = st;
   return rc;
+}
+}  // namespace
+
+NWG_API int nwg_msbfs(nwg_msbfs_ws h, const uint32_t* roots_host, uint32_t k, uint8_t* depths_dev, int alpha,
+                      void* stream, nwg_msbfs_stats* stats) {
+  NWG_GUARD_BEGIN
+  nwg_msbfs_stats st = {};
+  int rc = msbfs_common(h, roots_host, k, depths_dev, 1, nullptr, alpha, stream, &st);
+  if (rc == NWG_OK && st.deep_sources) {
+    st.status = rc = set_error(NWG_EOVERFLOW, std::to_string(st.deep_sources) +
+                                                  " source(s) reach depth 255 or more, beyond uint8: their rows hold "
+                                                  "the depths up to 254 (255 beyond); every other row is exact");
+  }
+  if (stats) *stats = st;
+  return rc;
+  NWG_GUARD_END
+}
+
+NWG_API int nwg_msbfs_ex(nwg_msbfs_ws h, const uint32_t* roots_host, uint32_t k, void* depths_dev,
+                         uint32_t depth_bytes, uint8_t* deep_flags_host, int alpha, void* stream,
+                         nwg_msbfs_stats* stats) {
+  NWG_GUARD_BEGIN
+  return msbfs_common(h, roots_host, k, depths_dev, depth_bytes, deep_flags_host, alpha, stream, stats);
   NWG_GUARD_END
 }
 

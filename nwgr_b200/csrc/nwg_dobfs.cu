@@ -1269,6 +1269,47 @@ __global__ void k_component(const uint64_t* __restrict__ off, const uint32_t* __
   }
 }
 
+// Depths from a parent array by pointer jumping (Wyllie's list ranking).
+// pair[v] = (ancestor << 32) | distance to it, starting at (parent, 1) and
+// (root, 0) for the root; unreached vertices hold ~0.  A round replaces
+// each pair by (ancestor's ancestor, sum of the two distances).  A pair is
+// read and written whole (one aligned 64-bit access), so any pair a thread
+// sees, updated this round or not, is a consistent (ancestor, distance) of
+// that vertex, and reading a newer one only shortens the remaining path:
+// after ceil(log2 n) + 1 rounds every reached vertex's ancestor is the root.
+__global__ void k_jump_init(const uint32_t* __restrict__ parents, uint64_t n, uint32_t root,
+                            unsigned long long* __restrict__ pair) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t par = parents[v];
+    pair[v] = par == kNull ? ~0ull : ((unsigned long long)par << 32) | (v == root ? 0u : 1u);
+  }
+}
+
+__global__ void k_jump_round(uint64_t n, unsigned long long* pair) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x) {
+    const unsigned long long pv = pair[v];
+    if (pv == ~0ull) continue;
+    const unsigned long long pa = pair[pv >> 32];
+    pair[v] = (pa & 0xFFFFFFFF00000000ull) | ((pv & 0xFFFFFFFFull) + (pa & 0xFFFFFFFFull));
+  }
+}
+
+// uint16 depth row from the jumped pairs: 0xFFFF = unreached; a depth that
+// does not fit below 0xFFFF sets *overflow.
+__global__ void k_jump_row16(const unsigned long long* __restrict__ pair, uint64_t n, uint16_t* __restrict__ row,
+                             int* overflow) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x) {
+    const unsigned long long pv = pair[v];
+    const uint64_t           d  = pv & 0xFFFFFFFFull;
+    if (pv == ~0ull) {
+      row[v] = 0xFFFF;
+    } else {
+      if (d >= 0xFFFF) *overflow = 1;
+      row[v] = (uint16_t)min(d, (uint64_t)0xFFFE);
+    }
+  }
+}
+
 __global__ void k_widen(const uint32_t* __restrict__ src, uint64_t* __restrict__ dst, uint64_t count) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (uint64_t)gridDim.x * blockDim.x)
     dst[i] = src[i];
@@ -1704,6 +1745,38 @@ int component_edges(GraphDev* g, const uint32_t* parents, uint64_t* edges, uint6
 int widen_offsets(const uint32_t* src, uint64_t* dst, uint64_t count, cudaStream_t stream) {
   k_widen<<<592, kThreads, 0, stream>>>(src, dst, count);
   NWG_CUDA_TRY(cudaGetLastError());
+  return NWG_OK;
+}
+
+// One single-source traversal on workspace ws (its graph) and the uint16
+// depth row of every vertex from its parents (row[v], 0xFFFF = unreached).
+// The pointer-jumping pairs use the workspace's small-queue buffers (2 n
+// uint32 entries), which the finished traversal no longer needs.  Returns
+// NWG_EOVERFLOW when a depth does not fit uint16.
+int depth_row16(Workspace* ws, uint32_t root, uint16_t* row, cudaStream_t stream) {
+  GraphDev* g = ws->g;
+  int       rc = ws_launch(ws, root, 15, 18, ws->parents, stream, false);
+  if (rc) return rc;
+  const uint64_t      n    = g->n;
+  unsigned long long* pair = reinterpret_cast<unsigned long long*>(ws->qbuf);
+  int* flag = reinterpret_cast<int*>(&ws->ctrl->err);  // the traversal's sticky error word, zero after a clean run
+  const int grid = grid_for(g, 4);
+  k_jump_init<<<grid, kThreads, 0, stream>>>(ws->parents, n, root, pair);
+  NWG_CUDA_TRY(cudaGetLastError());
+  int rounds = 1;
+  while ((1ull << (rounds - 1)) < n) ++rounds;  // ceil(log2 n) + 1
+  for (int r = 0; r < rounds; ++r) {
+    k_jump_round<<<grid, kThreads, 0, stream>>>(n, pair);
+    NWG_CUDA_TRY(cudaGetLastError());
+  }
+  k_jump_row16<<<grid, kThreads, 0, stream>>>(pair, n, row, flag);
+  NWG_CUDA_TRY(cudaGetLastError());
+  int32_t status[2] = {0, 0};
+  NWG_CUDA_TRY(cudaMemcpyAsync(&status[0], &ws->ctrl->h.status, sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+  NWG_CUDA_TRY(cudaMemcpyAsync(&status[1], flag, sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+  NWG_CUDA_TRY(cudaStreamSynchronize(stream));
+  if (status[0] != 0) return set_error(status[0], "single-source traversal of a deep source failed");
+  if (status[1] != 0) return set_error(NWG_EOVERFLOW, "a depth reaches 65535: does not fit the uint16 encoding");
   return NWG_OK;
 }
 

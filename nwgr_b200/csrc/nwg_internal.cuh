@@ -182,6 +182,8 @@ struct MsWorkspace {
   bool            stepped = false;      // host-driven levels (NWG_MS_STEPPED=1), for profilers
   cudaStream_t    stream  = nullptr;
   cudaEvent_t     ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t     ev_fork = nullptr;     // the caller's stream position that the lanes start after
+  std::vector<MsWorkspace*> lanes;       // further pass states for calls of more than one pass (own streams)
 };
 
 // Ragged batch (many small graphs, one persistent launch).
@@ -287,6 +289,7 @@ int  run_stepped(const DobfsParams& params, int sm_count, uint32_t root, int alp
                  cudaStream_t stream);
 int  zero_indegree_into(const uint64_t* in_off, uint64_t n, uint32_t* Z, int sm_count, cudaStream_t stream);
 void fill_stats(const Ctrl& c, nwg_bfs_stats* s);
+int  depth_row16(Workspace* ws, uint32_t root, uint16_t* row, cudaStream_t stream);
 int  build_zero_indegree(GraphDev* g, cudaStream_t stream);
 int  component_edges(GraphDev* g, const uint32_t* parents, uint64_t* edges, uint64_t* vertices);
 int  widen_offsets(const uint32_t* src, uint64_t* dst, uint64_t count, cudaStream_t stream);
@@ -300,10 +303,10 @@ int      ms_ws_init(GraphDev* g, MsWorkspace* ws);
 int      ms_ws_init_cap(GraphDev* g, uint64_t n_cap, uint64_t m_cap, MsWorkspace* ws);
 uint64_t ms_ws_bytes(uint64_t n_cap, uint64_t m_cap);
 void     ms_ws_free(MsWorkspace* ws);
-int      ms_run_on(MsWorkspace* ws, GraphDev* g, const uint32_t* roots_host, uint32_t k, uint8_t* depths_dev, int alpha,
-                   cudaStream_t stream, nwg_msbfs_stats* st);
-int  ms_run(MsWorkspace* ws, const uint32_t* roots_host, uint32_t k, uint8_t* depths_dev, int alpha, cudaStream_t stream,
-            nwg_msbfs_stats* st);
+int      ms_run_on(MsWorkspace* ws, GraphDev* g, const uint32_t* roots_host, uint32_t k, void* depths_dev,
+                   uint32_t depth_bytes, uint8_t* deep_flags, int alpha, cudaStream_t stream, nwg_msbfs_stats* st);
+int      ms_run(MsWorkspace* ws, const uint32_t* roots_host, uint32_t k, void* depths_dev, uint32_t depth_bytes,
+                uint8_t* deep_flags, int alpha, cudaStream_t stream, nwg_msbfs_stats* st);
 
 // nwg_gen.cu
 int gen_rmat(uint32_t scale, uint32_t ef, uint64_t seed, uint32_t ta, uint32_t tab, uint32_t tabc, GraphDev* g);

@@ -22,6 +22,7 @@
 // chosen like the single-source switch: pull when the frontier's out-edges
 // exceed the unexplored edges / alpha (nw::graph::bfs, bfs.hpp:186).
 #include <algorithm>
+#include <new>
 #include <cstdlib>
 #include <cstring>
 #include <vector>
@@ -66,6 +67,7 @@ struct MsPassDev {
   uint64_t   clear_max;   // ... and the frontier two levels back has at most this many chunk entries
   uint64_t   nclear;      // chunk entries of the frontier two levels back (still in list_nxt)
   uint32_t   sparse_ok;   // this push level finalizes sparsely
+  unsigned long long deep[4];  // sources that still discovered vertices at level 255 (their depths exceed uint8)
   MsCounters cnt[2];     // level L's kernels add into cnt[L & 1]
   uint32_t   roots[256], uniq[256];
   uint8_t    tr_pull[kMsTrace];
@@ -95,7 +97,8 @@ struct MsParams {
   uint64_t*        list_cur;  // frontier chunk entries (vertex << 32 | chunk), push input
   uint64_t*        list_nxt;
   uint64_t         list_cap;
-  uint8_t*         depth;     // [k][n], rows of this pass start at depth + src0 * n
+  uint8_t*         depth;     // [k][n] rows of depth_bytes each, this pass's first row at `depth`
+  uint32_t         depth_bytes;  // 1: uint8 rows (255 = unreached), 2: uint16 rows (0xFFFF = unreached)
   uint64_t         full[W];   // mask of the valid sources of each word
   MsCounters*      cnt;       // counters of the level being produced
   const MsCounters* prev;     // counters of the level before (its alive sources)
@@ -205,12 +208,25 @@ __device__ __forceinline__ void depth_tile(const MsParams<W>& p, int planes, uin
     for (int t = 0; t < 4; ++t) {
       if (s0 + t >= nsrc) break;
       const uint32_t row = __byte_perm(b[0], b[1], (uint32_t)(t | ((4 + t) << 4)));  // byte t of each vertex
-      uint8_t*       dst = p.depth + (uint64_t)(64 * w + s0 + t) * n + v0;
-      if (aligned && v0 + 1 < n) {
-        *reinterpret_cast<uint16_t*>(dst) = (uint16_t)row;
+      const uint64_t at  = (uint64_t)(64 * w + s0 + t) * n + v0;
+      if (p.depth_bytes == 2) {  // widen: 255 (unreached) -> 0xFFFF, any other depth d -> d
+        const uint32_t ff  = __vcmpeq4(row, 0xFFFFFFFFu);  // 0xFF in each byte that is 255
+        const uint32_t two = __byte_perm(row, ff, 0x5140);  // vertex v0 in the low half, v0 + 1 in the high half
+        uint16_t*      dst = reinterpret_cast<uint16_t*>(p.depth) + at;
+        if (aligned && v0 + 1 < n) {
+          *reinterpret_cast<uint32_t*>(dst) = two;
+        } else {
+          dst[0] = (uint16_t)two;
+          if (v0 + 1 < n) dst[1] = (uint16_t)(two >> 16);
+        }
       } else {
-        dst[0] = (uint8_t)row;
-        if (v0 + 1 < n) dst[1] = (uint8_t)(row >> 8);
+        uint8_t* dst = p.depth + at;
+        if (aligned && v0 + 1 < n) {
+          *reinterpret_cast<uint16_t*>(dst) = (uint16_t)row;
+        } else {
+          dst[0] = (uint8_t)row;
+          if (v0 + 1 < n) dst[1] = (uint8_t)(row >> 8);
+        }
       }
     }
   }
@@ -229,7 +245,8 @@ __global__ void __launch_bounds__(kMsThreads, 4) k_ms_depths(MsParams<W> p) {
   const uint64_t tiles  = (p.n + 63) / 64 * W;
   const uint64_t gwarp  = (uint64_t)blockIdx.x * kMsWarps + (threadIdx.x >> 5);
   const uint64_t nwarps = (uint64_t)gridDim.x * kMsWarps;
-  const bool     aligned = ((reinterpret_cast<uintptr_t>(p.depth) | p.n) & 1u) == 0;
+  // pairs of vertices are stored together when the rows keep them aligned
+  const bool     aligned = ((reinterpret_cast<uintptr_t>(p.depth) & (2u * p.depth_bytes - 1u)) | (p.n & 1u)) == 0;
   for (uint64_t t = gwarp; t < tiles; t += nwarps) {
     const int      w    = (int)(t % W);  // words of the same vertices in adjacent warps: shared VIS sectors
     const uint64_t v0   = (t / W) * 64 + lane * 2;
@@ -605,7 +622,9 @@ __global__ void k_ms_root_list(MsParams<W> p) {  // level 0: writes list[0] and 
 }
 
 // The level loop's decision, one thread, before every level: stop when the
-// level just run discovered nothing (or a depth would reach 255), else pull
+// level just run discovered nothing, or after level 255 (depths from 255 on
+// do not fit the level planes; the sources that still discovered vertices
+// at level 255 are recorded as deep, the others' depths are complete), else pull
 // when the frontier's out-edges exceed the unpushed edges / alpha
 // (nw::graph::bfs, bfs.hpp:186), push otherwise.  Records the per-level
 // trace; with set_cond it drives the graph's WHILE node and this parity's
@@ -628,7 +647,9 @@ __global__ void k_ms_decide(MsPassDev* d, cudaGraphConditionalHandle h_loop, cud
       if (prev.discovered == 0) stop = true;
       else d->levels = L;
     }
-    if (!stop && L >= 255) {
+    if (!stop && L >= 256) {
+#pragma unroll
+      for (int w = 0; w < 4; ++w) d->deep[w] = prev.alive[w];
       d->status = NWG_EOVERFLOW;
       stop      = true;
     }
@@ -695,7 +716,7 @@ struct MsArgs {
 };
 
 template <int W>
-MsArgs<W> ms_args(GraphDev* g, MsWorkspace* ws, uint8_t* depth_rows, uint32_t k) {
+MsArgs<W> ms_args(GraphDev* g, MsWorkspace* ws, uint8_t* depth_rows, uint32_t depth_bytes, uint32_t k) {
   MsArgs<W>    a;
   MsParams<W>& p = a.base;
   std::memset(&p, 0, sizeof p);
@@ -714,6 +735,7 @@ MsArgs<W> ms_args(GraphDev* g, MsWorkspace* ws, uint8_t* depth_rows, uint32_t k)
   p.plane    = g->n * W;
   p.list_cap = ws->list_cap;
   p.depth    = depth_rows;
+  p.depth_bytes = depth_bytes;
   for (int w = 0; w < W; ++w) {
     const int64_t bits = std::min<int64_t>(64, (int64_t)k - 64 * w);
     p.full[w]          = bits >= 64 ? ~0ull : bits <= 0 ? 0ull : ((1ull << bits) - 1);
@@ -878,7 +900,7 @@ int ms_prepare(MsWorkspace* ws) {
   GraphDev  empty;
   empty.n = 0;
   empty.m = 0;
-  MsArgs<W> a = ms_args<W>(&empty, ws, nullptr, 0);
+  MsArgs<W> a = ms_args<W>(&empty, ws, nullptr, 1, 0);
   return ms_build_exec<W>(ws, a);
 }
 
@@ -921,8 +943,8 @@ int ms_run_stepped(MsWorkspace* ws, MsArgs<W>& a, cudaStream_t stream) {
 // reads the record back once at the end.  Every byte of the k depth rows is
 // written by the pass's last kernel (no fill beforehand).
 template <int W>
-int ms_pass(GraphDev* g, MsWorkspace* ws, const uint32_t* roots_host, uint32_t k, uint8_t* depth_rows, int alpha,
-            cudaStream_t stream, nwg_msbfs_stats* st) {
+int ms_pass_launch(GraphDev* g, MsWorkspace* ws, const uint32_t* roots_host, uint32_t k, uint8_t* depth_rows,
+                   uint32_t depth_bytes, int alpha, cudaStream_t stream) {
   const uint64_t n  = g->n;
   MsPassDev&     h  = *static_cast<MsPassDev*>(ws->pass_host);
   MsPassDev*     dd = static_cast<MsPassDev*>(ws->pass_dev);
@@ -941,7 +963,7 @@ int ms_pass(GraphDev* g, MsWorkspace* ws, const uint32_t* roots_host, uint32_t k
   h.nuniq = (uint32_t)uniq.size();
   std::memcpy(h.uniq, uniq.data(), uniq.size() * sizeof(uint32_t));
 
-  MsArgs<W>    a     = ms_args<W>(g, ws, depth_rows, k);
+  MsArgs<W>    a     = ms_args<W>(g, ws, depth_rows, depth_bytes, k);
   const size_t words = (size_t)n * W * sizeof(uint64_t);
   NWG_CUDA_TRY(cudaMemsetAsync(ws->vis, 0, words, stream));
   NWG_CUDA_TRY(cudaMemsetAsync(ws->fr[0], 0, words, stream));
@@ -957,10 +979,21 @@ int ms_pass(GraphDev* g, MsWorkspace* ws, const uint32_t* roots_host, uint32_t k
     NWG_CUDA_TRY(cudaGraphLaunch(ws->exec[W - 1], stream));
   }
   NWG_CUDA_TRY(cudaMemcpyAsync(&h, dd, sizeof h, cudaMemcpyDeviceToHost, stream));
+  return NWG_OK;
+}
+
+// Waits for the pass launched on ws (on `stream`) and takes its record: the
+// deep sources (indices within the pass) and the statistics.
+int ms_pass_finish(MsWorkspace* ws, uint32_t k, std::vector<uint32_t>& deep, cudaStream_t stream,
+                   nwg_msbfs_stats* st) {
+  const MsPassDev& h = *static_cast<const MsPassDev*>(ws->pass_host);
   NWG_CUDA_TRY(cudaStreamSynchronize(stream));
-  if (h.status == NWG_EOVERFLOW)
-    return set_error(NWG_EOVERFLOW, "a depth reaches 255: does not fit the uint8 encoding");
-  if (h.status != NWG_OK) return set_error(h.status, "multi-source pass failed");
+  if (h.status == NWG_EOVERFLOW) {  // per source: the others' rows are complete
+    for (uint32_t i = 0; i < k; ++i)
+      if ((h.deep[i >> 6] >> (i & 63)) & 1ull) deep.push_back(i);
+  } else if (h.status != NWG_OK) {
+    return set_error(h.status, "multi-source pass failed");
+  }
   st->levels = std::max(st->levels, h.levels);
   st->push_levels += h.push_levels;
   st->pull_levels += h.pull_levels;
@@ -1017,6 +1050,7 @@ int ms_ws_init_cap(GraphDev* g, uint64_t n_cap, uint64_t m_cap, MsWorkspace* ws)
   NWG_CUDA_TRY(cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking));
   NWG_CUDA_TRY(cudaEventCreate(&ws->ev0));
   NWG_CUDA_TRY(cudaEventCreate(&ws->ev1));
+  NWG_CUDA_TRY(cudaEventCreateWithFlags(&ws->ev_fork, cudaEventDisableTiming));
   if (!ws->stepped) {
     int rc = ms_prepare<1>(ws);
     if (!rc) rc = ms_prepare<2>(ws);
@@ -1031,6 +1065,8 @@ int ms_ws_init(GraphDev* g, MsWorkspace* ws) { return ms_ws_init_cap(g, g->n, g-
 
 void ms_ws_free(MsWorkspace* ws) {
   if (!ws) return;
+  for (MsWorkspace* lane : ws->lanes) ms_ws_free(lane);
+  ws->lanes.clear();
   if (ws->stream) cudaStreamSynchronize(ws->stream);
   for (cudaGraphExec_t e : ws->exec)
     if (e) cudaGraphExecDestroy(e);
@@ -1049,42 +1085,122 @@ void ms_ws_free(MsWorkspace* ws) {
   if (ws->pass_host) cudaFreeHost(ws->pass_host);
   if (ws->ev0) cudaEventDestroy(ws->ev0);
   if (ws->ev1) cudaEventDestroy(ws->ev1);
+  if (ws->ev_fork) cudaEventDestroy(ws->ev_fork);
   if (ws->stream) cudaStreamDestroy(ws->stream);
   delete ws;
 }
 
+namespace {
+
+int ms_launch_any(GraphDev* g, MsWorkspace* ws, const uint32_t* roots, uint32_t kk, uint8_t* rows,
+                  uint32_t depth_bytes, int alpha, cudaStream_t s) {
+  if (kk <= 64) return ms_pass_launch<1>(g, ws, roots, kk, rows, depth_bytes, alpha, s);
+  if (kk <= 128) return ms_pass_launch<2>(g, ws, roots, kk, rows, depth_bytes, alpha, s);
+  if (kk <= 192) return ms_pass_launch<3>(g, ws, roots, kk, rows, depth_bytes, alpha, s);
+  return ms_pass_launch<4>(g, ws, roots, kk, rows, depth_bytes, alpha, s);
+}
+
+constexpr uint32_t kMsLanes = 4;  // passes of one call in flight at once
+
+}  // namespace
+
 // Runs ceil(k / 256) passes of up to 256 sources over graph g, which must
-// fit the workspace's capacity, on `stream` (or the workspace's own).
-int ms_run_on(MsWorkspace* ws, GraphDev* g, const uint32_t* roots_host, uint32_t k, uint8_t* depths_dev, int alpha,
-              cudaStream_t stream, nwg_msbfs_stats* st) {
+// fit the workspace's capacity, into k rows of depth_bytes (1 or 2) per
+// vertex.  The first pass runs on `stream` (or the workspace's own); with
+// more than one pass, up to kMsLanes passes are in flight at once, each on
+// a lane of its own (a second set of pass state and a stream, created on the
+// first such call and kept), which overlaps one pass's latency-bound levels
+// with the others'.  The lanes start after the work already on `stream`
+// and `stream` waits for them, so the call keeps its stream order.
+//
+// A source whose traversal goes deeper than level 254 does not fail the
+// pass: the other sources' rows are complete, and that source is counted in
+// st->deep_sources and flagged in deep_flags[i] (k bytes; may be null).
+// With uint16 rows its row is then computed exactly by one single-source
+// traversal on a workspace made for the purpose and freed again (such
+// sources are rare: a graph whose diameter passes 254); with uint8 rows it
+// keeps the depths up to 254 and 255 beyond.
+int ms_run_on(MsWorkspace* ws, GraphDev* g, const uint32_t* roots_host, uint32_t k, void* depths_dev,
+              uint32_t depth_bytes, uint8_t* deep_flags, int alpha, cudaStream_t stream, nwg_msbfs_stats* st) {
   if (g->n > ws->n_cap || g->m > ws->m_cap)
     return set_error(NWG_EINVAL, "graph larger than the multi-source workspace's capacity");
   for (uint32_t i = 0; i < k; ++i)
     if (roots_host[i] >= g->n) return set_error(NWG_EINVAL, "root " + std::to_string(roots_host[i]) + " >= n");
   if (alpha <= 0) return set_error(NWG_EINVAL, "alpha must be positive");
-  cudaStream_t s = stream ? stream : ws->stream;
-  for (uint32_t b = 0; b < k; b += 256) {
-    const uint32_t kk = std::min<uint32_t>(256, k - b);
-    uint8_t* rows = depths_dev + (uint64_t)b * g->n;
-    int      rc;
-    if (kk <= 64) {
-      rc = ms_pass<1>(g, ws, roots_host + b, kk, rows, alpha, s, st);
-    } else if (kk <= 128) {
-      rc = ms_pass<2>(g, ws, roots_host + b, kk, rows, alpha, s, st);
-    } else if (kk <= 192) {
-      rc = ms_pass<3>(g, ws, roots_host + b, kk, rows, alpha, s, st);
-    } else {
-      rc = ms_pass<4>(g, ws, roots_host + b, kk, rows, alpha, s, st);
+  if (depth_bytes != 1 && depth_bytes != 2) return set_error(NWG_EINVAL, "depth rows must have 1 or 2 bytes per vertex");
+  if (deep_flags) std::memset(deep_flags, 0, k);
+  cudaStream_t   s       = stream ? stream : ws->stream;
+  const uint32_t npasses = (k + 255) / 256;
+  const uint32_t nlanes  = std::min(npasses, kMsLanes);
+  // lane 0 is the workspace itself on `s`; the others wait for `s`'s prior work
+  while (ws->lanes.size() + 1 < nlanes) {
+    auto* lane = new (std::nothrow) MsWorkspace();
+    if (!lane) return set_error(NWG_ENOMEM, "host allocation failed");
+    const int rc = ms_ws_init_cap(ws->g, ws->n_cap, ws->m_cap, lane);
+    if (rc) {
+      ms_ws_free(lane);
+      return rc;
     }
-    if (rc) return rc;
-    st->passes++;
+    ws->lanes.push_back(lane);
   }
-  return NWG_OK;
+  auto lane_ws     = [&](uint32_t l) { return l == 0 ? ws : ws->lanes[l - 1]; };
+  auto lane_stream = [&](uint32_t l) { return l == 0 ? s : ws->lanes[l - 1]->stream; };
+  if (nlanes > 1) {
+    NWG_CUDA_TRY(cudaEventRecord(ws->ev_fork, s));
+    for (uint32_t l = 1; l < nlanes; ++l) NWG_CUDA_TRY(cudaStreamWaitEvent(lane_stream(l), ws->ev_fork, 0));
+  }
+  std::vector<uint32_t> deep;
+  Workspace*            single = nullptr;  // single-source traversals of deep sources (uint16 rows only)
+  int                   rc     = NWG_OK;
+  auto rows_of = [&](uint32_t p) {
+    return static_cast<uint8_t*>(depths_dev) + (uint64_t)p * 256 * g->n * depth_bytes;
+  };
+  // pass p runs on lane p % nlanes; before a lane takes a pass it finishes
+  // its previous one (p - nlanes), so passes finish in order
+  auto finish = [&](uint32_t p) -> int {
+    const uint32_t l  = p % nlanes;
+    const uint32_t kk = std::min<uint32_t>(256, k - 256 * p);
+    deep.clear();
+    int r = ms_pass_finish(lane_ws(l), kk, deep, lane_stream(l), st);
+    if (r) return r;
+    st->passes++;
+    for (uint32_t i : deep) {
+      st->deep_sources++;
+      if (deep_flags) deep_flags[256 * p + i] = 1;
+      if (depth_bytes != 2) continue;
+      if (!single) {
+        single = new (std::nothrow) Workspace();
+        if (!single) return set_error(NWG_ENOMEM, "host allocation failed");
+        if ((r = ws_init(g, single)) != NWG_OK) return r;
+      }
+      r = depth_row16(single, roots_host[256 * p + i], reinterpret_cast<uint16_t*>(rows_of(p)) + (uint64_t)i * g->n,
+                      lane_stream(l));
+      if (r) return r;
+    }
+    return NWG_OK;
+  };
+  uint32_t done = 0;  // passes finished
+  for (uint32_t p = 0; p < npasses && rc == NWG_OK; ++p) {
+    if (p >= nlanes && (rc = finish(done++)) != NWG_OK) break;
+    const uint32_t l  = p % nlanes;
+    const uint32_t kk = std::min<uint32_t>(256, k - 256 * p);
+    rc = ms_launch_any(g, lane_ws(l), roots_host + 256 * p, kk, rows_of(p), depth_bytes, alpha, lane_stream(l));
+  }
+  while (done < npasses) {  // after an error, what was launched still completes before the call returns
+    const int r = finish(done++);
+    if (rc == NWG_OK) rc = r;
+  }
+  for (uint32_t l = 1; l < nlanes; ++l) {  // `s` continues after every lane's work
+    cudaEventRecord(ws->lanes[l - 1]->ev0, lane_stream(l));
+    cudaStreamWaitEvent(s, ws->lanes[l - 1]->ev0, 0);
+  }
+  if (single) ws_free(single);
+  return rc;
 }
 
-int ms_run(MsWorkspace* ws, const uint32_t* roots_host, uint32_t k, uint8_t* depths_dev, int alpha,
-           cudaStream_t stream, nwg_msbfs_stats* st) {
-  return ms_run_on(ws, ws->g, roots_host, k, depths_dev, alpha, stream, st);
+int ms_run(MsWorkspace* ws, const uint32_t* roots_host, uint32_t k, void* depths_dev, uint32_t depth_bytes,
+           uint8_t* deep_flags, int alpha, cudaStream_t stream, nwg_msbfs_stats* st) {
+  return ms_run_on(ws, ws->g, roots_host, k, depths_dev, depth_bytes, deep_flags, alpha, stream, st);
 }
 
 }  // namespace nwg

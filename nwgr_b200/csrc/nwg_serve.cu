@@ -1,5 +1,6 @@
 // Serving loop: (graph, root) BFS queries against graphs kept resident in
-// HBM, answered as uint8 depth rows (255 = unreached).  No reference
+// HBM, answered as depth rows: uint8 (255 = unreached) or, with
+// depth_bytes = 2, uint16 (0xFFFF = unreached).  No reference
 // counterpart: NWGraph answers one bfs call at a time; each answer here equals
 // the single-source BFS depths of that (graph, root).
 //
@@ -45,7 +46,7 @@ constexpr uint32_t kMaxBatch = 256;  // sources of one multi-source pass
 
 struct Query {
   uint32_t          graph = 0, root = 0;
-  uint8_t*          out   = nullptr;  // host destination (n of the graph) or null
+  uint8_t*          out   = nullptr;  // host destination (n * depth_bytes bytes of the graph) or null
   uint64_t          bytes = 0;        // per-query state while taken
   Clock::time_point arrival{}, done_at{};
   uint32_t          batch  = 0;       // size of the batch it ran in
@@ -56,8 +57,8 @@ struct Query {
 
 struct Slot {
   MsWorkspace* ws        = nullptr;
-  uint8_t*     depth_dev = nullptr;  // kMaxBatch * n_cap
-  uint8_t*     staging   = nullptr;  // pinned, kMaxBatch * n_cap
+  uint8_t*     depth_dev = nullptr;  // kMaxBatch * n_cap * depth_bytes
+  uint8_t*     staging   = nullptr;  // pinned, the same size
   std::thread  th;
 };
 
@@ -67,6 +68,7 @@ struct Server {
   uint32_t                max_batch = kMaxBatch;
   uint64_t                budget    = 0;
   int                     alpha     = 4;
+  uint32_t                depth_bytes = 1;  // bytes per vertex of an answer row
   uint64_t                n_cap = 0, m_cap = 0, slot_bytes = 0;
   std::vector<Slot>       slots;
   std::mutex              mu;
@@ -84,10 +86,10 @@ struct Server {
   std::string first_error;
 };
 
-// State a query holds while a slot works on it: its uint8 depth row on the
-// device and in pinned host memory, and one bit per vertex in each of the
-// pass's four bitsets (VIS, FR[2], NX).
-uint64_t query_bytes(uint64_t n) { return 2 * n + (4 * n + 7) / 8; }
+// State a query holds while a slot works on it: its depth row on the device
+// and in pinned host memory, and one bit per vertex in each of the pass's
+// four bitsets (VIS, FR[2], NX).
+uint64_t query_bytes(uint64_t n, uint32_t depth_bytes) { return 2 * n * depth_bytes + (4 * n + 7) / 8; }
 
 Query* oldest_waiting(Server* s) {
   while (!s->fifo.empty() && s->fifo.front()->taken) s->fifo.pop_front();
@@ -98,6 +100,7 @@ void worker(Server* s, Slot* slot) {
   cudaSetDevice(s->device);
   std::vector<Query*>   batch;
   std::vector<uint32_t> roots;
+  std::vector<uint8_t>  deep(kMaxBatch);
   batch.reserve(kMaxBatch);
   roots.reserve(kMaxBatch);
   for (;;) {
@@ -129,35 +132,41 @@ void worker(Server* s, Slot* slot) {
     const auto k      = (uint32_t)batch.size();
     roots.clear();
     for (Query* q : batch) roots.push_back(q->root);
-    nwg_msbfs_stats st = {};
-    int             rc = ms_run_on(slot->ws, g, roots.data(), k, slot->depth_dev, s->alpha, slot->ws->stream, &st);
+    nwg_msbfs_stats st   = {};
+    const size_t    row  = (size_t)g->n * s->depth_bytes;
+    int rc = ms_run_on(slot->ws, g, roots.data(), k, slot->depth_dev, s->depth_bytes, deep.data(), s->alpha,
+                       slot->ws->stream, &st);
     if (rc == NWG_OK) {
-      cudaError_t e = cudaMemcpyAsync(slot->staging, slot->depth_dev, (size_t)k * g->n, cudaMemcpyDeviceToHost,
+      cudaError_t e = cudaMemcpyAsync(slot->staging, slot->depth_dev, k * row, cudaMemcpyDeviceToHost,
                                       slot->ws->stream);
       if (e == cudaSuccess) e = cudaStreamSynchronize(slot->ws->stream);
       if (e != cudaSuccess) rc = cuda_error(e, "serving batch read-back");
     }
     if (rc == NWG_OK)
       for (uint32_t i = 0; i < k; ++i)
-        if (batch[i]->out) std::memcpy(batch[i]->out, slot->staging + (size_t)i * g->n, g->n);
+        if (batch[i]->out) std::memcpy(batch[i]->out, slot->staging + i * row, row);
     std::string err;
     if (rc != NWG_OK) {
       char buf[512];
       nwg_last_error(buf, sizeof buf);
       err = buf;
+    } else if (st.deep_sources) {  // only uint8 answers can be deep: those queries alone fail
+      err = "a query's traversal goes deeper than 254 levels: its uint8 answer holds the depths up to 254 and "
+            "255 beyond (depth_bytes = 2 answers it exactly)";
     }
     const auto t_done = Clock::now();
 
     lk.lock();
-    for (Query* q : batch) {
+    for (uint32_t i = 0; i < k; ++i) {
+      Query* q   = batch[i];
       q->done_at = t_done;
       q->batch   = k;
-      q->status  = rc;
+      q->status  = (rc == NWG_OK && s->depth_bytes == 1 && deep[i]) ? NWG_EOVERFLOW : rc;
       q->done    = true;
       if (q->group_done) ++*q->group_done;
       s->in_use -= q->bytes;
     }
-    if (rc != NWG_OK && s->first_error.empty()) s->first_error = err;
+    if (!err.empty() && s->first_error.empty()) s->first_error = err;
     s->in_flight--;
     s->batches++;
     s->done_count += k;
@@ -196,7 +205,7 @@ int check_query(const Server* s, uint32_t graph, uint32_t root, uint32_t i) {
   if (graph >= s->graphs.size())
     return set_error(NWG_EINVAL, "query " + std::to_string(i) + ": graph index out of range");
   if (root >= s->graphs[graph]->n) return set_error(NWG_EINVAL, "query " + std::to_string(i) + ": root >= n");
-  if (query_bytes(s->graphs[graph]->n) > s->budget)
+  if (query_bytes(s->graphs[graph]->n, s->depth_bytes) > s->budget)
     return set_error(NWG_EINVAL, "query " + std::to_string(i) + ": its state alone exceeds the budget");
   return NWG_OK;
 }
@@ -229,7 +238,9 @@ NWG_API int nwg_server_create(const nwg_graph* graphs, uint32_t num_graphs, cons
     if (want_slots > 64) return set_error(NWG_EINVAL, "slots must be 1..64");
     if (max_batch > kMaxBatch) return set_error(NWG_EINVAL, "max_batch must be 1..256");
     if (c.alpha < 0) return set_error(NWG_EINVAL, "alpha must be positive");
+    if (c.depth_bytes > 2) return set_error(NWG_EINVAL, "depth_bytes must be 1 or 2");
     auto* s      = new Server();
+    s->depth_bytes = c.depth_bytes ? c.depth_bytes : 1;
     s->max_batch = max_batch;
     s->budget    = c.budget_bytes ? c.budget_bytes : (16ull << 30);
     s->alpha     = c.alpha ? c.alpha : 4;
@@ -249,10 +260,12 @@ NWG_API int nwg_server_create(const nwg_graph* graphs, uint32_t num_graphs, cons
       s->m_cap = std::max(s->m_cap, g->m);
     }
     s->per_graph.resize(num_graphs);
-    s->slot_bytes = ms_ws_bytes(s->n_cap, s->m_cap) + 2ull * kMaxBatch * std::max<uint64_t>(s->n_cap, 1);
+    const uint64_t rows_bytes = (uint64_t)kMaxBatch * std::max<uint64_t>(s->n_cap, 1) * s->depth_bytes;
+    s->slot_bytes = ms_ws_bytes(s->n_cap, s->m_cap) + 2ull * rows_bytes;
     // the slots' fixed buffers count against the budget; keep room for at
     // least one largest query beside them
-    const uint64_t room = s->budget > query_bytes(s->n_cap) ? s->budget - query_bytes(s->n_cap) : 0;
+    const uint64_t biggest = query_bytes(s->n_cap, s->depth_bytes);
+    const uint64_t room    = s->budget > biggest ? s->budget - biggest : 0;
     const uint64_t fit  = room / s->slot_bytes;
     if (fit == 0) {
       delete s;
@@ -268,8 +281,8 @@ NWG_API int nwg_server_create(const nwg_graph* graphs, uint32_t num_graphs, cons
     for (Slot& sl : s->slots) {
       sl.ws  = new MsWorkspace();
       int rc = ms_ws_init_cap(nullptr, s->n_cap, s->m_cap, sl.ws);
-      if (rc == NWG_OK && (cudaMalloc(&sl.depth_dev, (size_t)kMaxBatch * s->n_cap) != cudaSuccess ||
-                           cudaMallocHost(&sl.staging, (size_t)kMaxBatch * s->n_cap) != cudaSuccess)) {
+      if (rc == NWG_OK && (cudaMalloc(&sl.depth_dev, (size_t)rows_bytes) != cudaSuccess ||
+                           cudaMallocHost(&sl.staging, (size_t)rows_bytes) != cudaSuccess)) {
         cudaGetLastError();
         rc = set_error(NWG_ENOMEM, "serving slot allocation failed");
       }
@@ -304,7 +317,7 @@ NWG_API int nwg_server_submit(nwg_server h, uint32_t graph, uint32_t root, uint8
   q->graph   = graph;
   q->root    = root;
   q->out     = depths_host;
-  q->bytes   = query_bytes(s->graphs[graph]->n);
+  q->bytes   = query_bytes(s->graphs[graph]->n, s->depth_bytes);
   q->heap    = true;
   q->arrival = Clock::now();
   {
@@ -353,7 +366,7 @@ NWG_API int nwg_server_run_trace(nwg_server h, uint32_t count, const uint32_t* g
       qs[i].graph = graph[i];
       qs[i].root  = root[i];
       qs[i].out   = depths_host ? depths_host[i] : nullptr;
-      qs[i].bytes = query_bytes(s->graphs[graph[i]]->n);
+      qs[i].bytes = query_bytes(s->graphs[graph[i]]->n, s->depth_bytes);
     }
     uint64_t b0;
     double   bt0;

@@ -126,3 +126,68 @@ def test_server_argument_errors(nwg, served):
     with pytest.raises(nwg.NwgError) as e:
         nwg.Server(graphs, budget_bytes=1 << 20)  # no slot fits
     assert "budget" in str(e.value)
+
+
+def path_plus_rmat(path_n):
+    """A path of path_n vertices beside an RMAT-10 graph (ids from path_n on)."""
+    u = np.arange(path_n - 1, dtype=np.uint64)
+    roff, rcols = gg.rmat(10, 16, seed=3)
+    ru = np.repeat(np.arange(roff.size - 1, dtype=np.uint64), (roff[1:] - roff[:-1]).astype(np.int64))
+    pu = np.concatenate([u, ru + np.uint64(path_n)])
+    pv = np.concatenate([u + np.uint64(1), rcols.astype(np.uint64) + np.uint64(path_n)])
+    return gg.csr_from_pairs(pu, pv, path_n + roff.size - 1)
+
+
+def test_deep_query_fails_alone_and_uint16_answers_it(nwg, port):
+    """A path graph of 600 vertices (depths up to 599) served beside RMAT
+    graphs and beside a graph holding both a 400-vertex path and an RMAT
+    component.  uint8 answers: only the queries whose depths reach 255 fail
+    (NWG_EOVERFLOW); every other query, including those coalesced with a
+    deep one into the same pass, is answered exactly.  uint16 answers:
+    every query is answered exactly and none fails."""
+    pn = 600
+    u = np.arange(pn - 1, dtype=np.uint64)
+    host = [gg.csr_from_pairs(u, u + np.uint64(1), pn), gg.rmat(11, 16, seed=8), gg.rmat(12, 8, seed=9),
+            path_plus_rmat(400)]
+    graphs = [nwg.Graph.from_csr(*h) for h in host]
+    queries = [(0, 0), (0, 300), (0, 599), (3, 0), (3, 200), (3, None), (3, 399), (0, 450), (1, None), (2, None),
+               (3, None), (0, 100), (1, None), (3, 150)]
+    rng = np.random.default_rng(3)
+    qs = []
+    for gi, r in queries:
+        if r is None:  # a root with out-edges in the RMAT part
+            base = 400 if gi == 3 else 0
+            r = base + int(gg.roots(host[gi][0][base:] - host[gi][0][base], 1, seed=int(rng.integers(1, 1000)))[0])
+        qs.append((gi, r))
+    want = [port.depths(host[gi][0], host[gi][1], r) for gi, r in qs]
+    deep = [int(np.where(w == NULL, 0, w).max()) >= 255 for w in want]
+    assert any(deep) and not all(deep)
+
+    # uint8 answers: submitted together, so each graph's queries share passes
+    srv = nwg.Server(graphs, slots=1, max_batch=256)
+    outs, tickets = [], []
+    for gi, r in qs:
+        outs.append(np.zeros(host[gi][0].size - 1, np.uint8))
+        tickets.append(srv.submit(gi, r, outs[-1]))
+    for i, t in enumerate(tickets):
+        if deep[i]:
+            with pytest.raises(nwg.NwgError) as e:
+                srv.wait(t)
+            assert e.value.code == nwg.NWG_EOVERFLOW
+        else:
+            srv.wait(t)
+            assert np.array_equal(outs[i], _u8(want[i])), qs[i]
+    srv.close()
+
+    # uint16 answers, replayed as a trace: all exact, none failed
+    srv = nwg.Server(graphs, slots=2, max_batch=256, depth_bytes=2)
+    gid = np.array([q[0] for q in qs], np.uint32)
+    roots = np.array([q[1] for q in qs], np.uint32)
+    outs = [np.zeros(host[gi][0].size - 1, np.uint16) for gi, _ in qs]
+    _, bs, st = srv.run_trace(gid, roots, np.zeros(len(qs)), outs)
+    assert st.failed == 0 and bs.max() > 1
+    for i in range(len(qs)):
+        assert np.array_equal(outs[i], np.where(want[i] == NULL, 0xFFFF, want[i]).astype(np.uint16)), qs[i]
+    srv.close()
+    for g in graphs:
+        g.release()
