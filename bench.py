@@ -396,7 +396,10 @@ def bench_ragged(nwg, torch, num_graphs=1000, reps=3):
             "total_entries": int(sum(m for _, m in mn)), "persistent_ms": t,
             "gteps": e_total / 2.0 / (t * 1e-3) / 1e9, "per_call_device_ms_sum": per_call_ms,
             "speedup_vs_per_call": per_call_ms / t, "blocks_per_sm": bps,
-            "classes": {k: v.__dict__ for k, v in params.items()}, "generate_s": gen_s, "autotune_s": tune_s}
+            "classes": len(params),
+            "warp_min_per_class": {str(w): sum(1 for v in params.values() if v.warp_min == w)
+                                   for w in sorted({v.warp_min for v in params.values()})},
+            "generate_s": gen_s, "autotune_s": tune_s}
 
 
 def profile_extension(args, torch):
@@ -512,11 +515,12 @@ def bench_serving(nwg, num_graphs=200, rates=SERVE_RATES, seconds=1.5, slots=16,
         count = int(max(2000, min(300000, rate * seconds)))
         gid, roots, arr = query_trace(pools, rate, count, seed=int(rate) % 1000003)
         _, bs, st = server.run_trace(gid, roots, arr)
-        out.append({"offered_qps": rate, "queries": count, "qps": st.qps, "p50_ms": st.p50_ms, "p99_ms": st.p99_ms,
-                    "max_ms": st.max_ms, "mean_batch": st.mean_batch, "batches": int(st.batches),
+        out.append({"offered_qps": rate, "queries": count, "qps": round(st.qps, 1), "p50_ms": round(st.p50_ms, 3),
+                    "p99_ms": round(st.p99_ms, 3), "max_ms": round(st.max_ms, 3),
+                    "mean_batch": round(st.mean_batch, 2), "failed": int(st.failed),
                     "peak_in_flight": int(st.peak_in_flight),
-                    "overlap": st.batch_time_s / st.wall_s if st.wall_s > 0 else 0.0,
-                    "peak_state_bytes": int(st.peak_state_bytes), "answer_bytes": int(sum(graphs[g].n for g in gid))})
+                    "overlap": round(st.batch_time_s / st.wall_s, 2) if st.wall_s > 0 else 0.0,
+                    "peak_state_mb": round(st.peak_state_bytes / 1e6, 1)})
     info = {"slots": int(st.slots), "slot_bytes": int(st.slot_bytes), "state_budget_bytes": int(st.budget_bytes)}
     server.close()
     for g in graphs:
@@ -714,7 +718,7 @@ def main():
         col_p = torch.from_numpy(cols.view(np.int32)).pin_memory()
         par_h = torch.empty(n, dtype=torch.int32).pin_memory()
         h2d = off.nbytes + cols.nbytes
-        e2e_vals = []
+        e2e_vals, ups, calls = [], [], []
         for step in range(1 + args.steps):
             t_up = time.perf_counter()
             ge = nwg.Graph.from_csr(off_p.numpy().view(np.uint64), col_p.numpy().view(np.uint32))
@@ -723,14 +727,37 @@ def main():
             for r in roots:
                 t1 = time.perf_counter()
                 nwg.bfs(ge, ge, int(r), parents_out=par_h.numpy().view(np.uint32))
-                ts.append(time.perf_counter() - t1 + up / len(roots))
+                ts.append(time.perf_counter() - t1)
             ge.release()
             if step > 0:
-                e2e_vals.append(hmean((e_r / 2.0) / np.asarray(ts) / 1e9))
+                e2e_vals.append(hmean((e_r / 2.0) / (np.asarray(ts) + up / len(roots)) / 1e9))
+                ups.append(up)
+                calls.extend(ts)
+        # the copies alone, for the split of the call time: one parent array
+        # device -> pinned host, and the CSR host -> device
+        d2h_s, h2d_s = [], []
+        for _ in range(5):
+            ta = time.perf_counter()
+            par_h.copy_(parents)
+            torch.cuda.synchronize()
+            d2h_s.append(time.perf_counter() - ta)
+        off_d = torch.empty(off.size, dtype=torch.int64, device="cuda")
+        col_d = torch.empty(cols.size, dtype=torch.int32, device="cuda")
+        for _ in range(2):
+            ta = time.perf_counter()
+            off_d.copy_(off_p)
+            col_d.copy_(col_p)
+            torch.cuda.synchronize()
+            h2d_s.append(time.perf_counter() - ta)
+        del off_d, col_d
         e2e = {"value": float(np.mean(e2e_vals)) * world, "unit": "GTEPS", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(4 * n * len(roots)),
-               "note": "per step: upload CSR from pinned host memory, 64 nwg_bfs calls each returning parents "
-                       "to pinned host memory, release"}
+               "upload_s_median": float(np.median(ups)), "upload_gbs": h2d / float(np.median(ups)) / 1e9,
+               "h2d_copy_gbs": h2d / min(h2d_s) / 1e9, "d2h_copy_gbs": 4.0 * n / min(d2h_s) / 1e9,
+               "d2h_copy_ms": 1e3 * min(d2h_s), "call_ms_median": 1e3 * float(np.median(calls)),
+               "note": "per step: upload CSR from pinned host memory (registration), 64 nwg_bfs calls each "
+                       "returning parents to pinned host memory, release; *_copy_gbs: the same bytes copied "
+                       "alone (one parent array, one CSR)"}
     verifier = None
     if not args.no_verify:
         verifier = bench_verifier(nwg, torch, g, roots, rank == 0 and not args.no_cpu)
@@ -796,8 +823,8 @@ def main():
                          "traffic_note": "ncu DRAM bytes of one traversal of the same graph kind at scale 22, "
                                          "scaled by directed entries" if traffic else None},
             "gpu_launches": int(np.sum(launches)) * args.steps,
-            "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, "batched": batched, "ragged": ragged,
-            "serving": serving, "verifier": verifier, "betweenness": bc, "other_graphs": other,
+            "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, "other_graphs": other, "verifier": verifier,
+            "betweenness": bc, "ragged": ragged, "batched": batched, "serving": serving,
         }
         print(json.dumps(line), flush=True)
     if ws is not None:
