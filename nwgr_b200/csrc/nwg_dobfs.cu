@@ -53,7 +53,7 @@ constexpr int kSmallBlocks = 64;  // grid of the small-frontier top-down branch
 constexpr int kClusterCtas = 8;   // the tiny-frontier branch: one cluster of this many blocks
 constexpr int kClusterUnits = kClusterCtas * (kThreads / 32);  // its work-unit limit: one per warp
 constexpr int kVisit       = 4;   // edges a lane claims per batch
-constexpr int kTdPerSm     = 3;   // k_td blocks per SM (80 registers per thread: 3 x 256 threads fill an SM)
+constexpr int kTdPerSm     = 4;   // k_td blocks per SM (64 registers per thread, no spills: 3% faster than 3 on the grid)
 
 __device__ __forceinline__ unsigned long long globaltimer() {
   unsigned long long t;
@@ -95,6 +95,24 @@ __host__ __device__ __forceinline__ uint64_t chunks_of(uint64_t deg, const Thres
 
 constexpr uint64_t kLaneChunks = 8;  // a lane writes up to this many chunk entries of one vertex itself
 
+// What one step of the traversal reads and where it adds its counts.  The
+// level-loop kernels take it from the control header; the persistent
+// traversal kernel from its own copy of the decision state and the step's
+// counter slot.
+struct StepView {
+  uint32_t*           parents;
+  uint32_t            in;       // queue buffer a top-down step expands
+  uint32_t            out;      // queue buffer a step appends to
+  uint64_t            nS, nC;   // small and chunk entries of the input queues
+  uint32_t            bu_mode;  // pull: 0 = front is V, 1 = front is the previous pull's discoveries
+  uint32_t            bm;       // pull: index of the discovery bitmap of the previous pull
+  unsigned long long* qpos;     // output queues' entries: small | chunk << 32
+  uint32_t*           qbig;     // chunked vertices appended
+  uint32_t*           nhub;     // deferred hub records appended
+  unsigned long long* scout;    // out-degree sum of the vertices a top-down step discovers
+  unsigned long long* awake;    // vertices a pull discovers
+};
+
 // ---------------------------------------------------------------------------
 // Appending discovered vertices to the next queue buffer `qi`.
 //
@@ -133,9 +151,9 @@ __device__ __forceinline__ void count_entries(const DobfsParams& p, const uint64
 // bound by its outstanding-store limit.  Otherwise the whole warp writes them,
 // 32 at a time.
 template <int K, bool kDefer>
-__device__ __forceinline__ void write_entries(const DobfsParams& p, uint32_t qi, const uint32_t (&v)[K],
+__device__ __forceinline__ void write_entries(const DobfsParams& p, const StepView& sv, const uint32_t (&v)[K],
                                               const uint64_t (&d)[K], uint32_t mask, uint64_t spos, uint64_t cpos) {
-  CtrlHdr*        c    = &p.ctrl->h;
+  const uint32_t  qi   = sv.out;
   const unsigned  lane = threadIdx.x & 31;
   uint32_t* const qs   = p.qs[qi];
   uint64_t* const qc   = p.qc[qi];
@@ -181,7 +199,7 @@ __device__ __forceinline__ void write_entries(const DobfsParams& p, uint32_t qi,
     }
     const uint32_t tot  = __shfl_sync(kFullMask, incl, 31);
     uint32_t       base = 0;
-    if (tot && lane == 31) base = atomicAdd(&c->nhub[qi], tot);
+    if (tot && lane == 31) base = atomicAdd(sv.nhub, tot);
     base         = __shfl_sync(kFullMask, base, 31);
     uint64_t idx = base + incl - nh;
     uint64_t pos = c0;
@@ -226,11 +244,11 @@ __device__ __forceinline__ void write_entries(const DobfsParams& p, uint32_t qi,
       }
     }
   }
-  if (over) c->status = NWG_EOVERFLOW;
+  if (over) atomicCAS(&p.ctrl->err, 0, NWG_EOVERFLOW);
 }
 
 template <int K, bool kDefer>
-__device__ __forceinline__ void append_warp(const DobfsParams& p, uint32_t qi, const uint32_t (&v)[K],
+__device__ __forceinline__ void append_warp(const DobfsParams& p, const StepView& sv, const uint32_t (&v)[K],
                                             const uint64_t (&d)[K], uint32_t mask, uint32_t& nbig) {
   uint32_t ns, nch, nb;
   count_entries<K>(p, d, mask, ns, nch, nb);
@@ -240,10 +258,10 @@ __device__ __forceinline__ void append_warp(const DobfsParams& p, uint32_t qi, c
   const unsigned long long tot  = __shfl_sync(kFullMask, incl, 31);
   if (tot == 0) return;
   unsigned long long base = 0;
-  if ((threadIdx.x & 31) == 31) base = atomicAdd(&p.ctrl->h.qpos[qi], tot);
+  if ((threadIdx.x & 31) == 31) base = atomicAdd(sv.qpos, tot);
   base                          = __shfl_sync(kFullMask, base, 31);
   const unsigned long long excl = incl - mine;
-  write_entries<K, kDefer>(p, qi, v, d, mask, (base & 0xFFFFFFFFull) + (excl & 0xFFFFFFFFull),
+  write_entries<K, kDefer>(p, sv, v, d, mask, (base & 0xFFFFFFFFull) + (excl & 0xFFFFFFFFull),
                            (base >> 32) + (excl >> 32));
 }
 
@@ -268,7 +286,7 @@ __device__ __forceinline__ unsigned long long block_excl_scan(unsigned long long
 }
 
 template <int K, bool kDefer>
-__device__ __forceinline__ void append_block(const DobfsParams& p, uint32_t qi, const uint32_t (&v)[K],
+__device__ __forceinline__ void append_block(const DobfsParams& p, const StepView& sv, const uint32_t (&v)[K],
                                              const uint64_t (&d)[K], uint32_t mask, uint32_t& nbig) {
   __shared__ unsigned long long s_base;
   uint32_t                      ns, nch, nb;
@@ -278,10 +296,10 @@ __device__ __forceinline__ void append_block(const DobfsParams& p, uint32_t qi, 
   unsigned long long       tot  = 0;
   const unsigned long long excl = block_excl_scan(mine, tot);
   if (tot == 0) return;  // block-uniform
-  if (threadIdx.x == 0) s_base = atomicAdd(&p.ctrl->h.qpos[qi], tot);
+  if (threadIdx.x == 0) s_base = atomicAdd(sv.qpos, tot);
   __syncthreads();
   const unsigned long long base = s_base;
-  write_entries<K, kDefer>(p, qi, v, d, mask, (base & 0xFFFFFFFFull) + (excl & 0xFFFFFFFFull),
+  write_entries<K, kDefer>(p, sv, v, d, mask, (base & 0xFFFFFFFFull) + (excl & 0xFFFFFFFFull),
                            (base >> 32) + (excl >> 32));
   __syncthreads();
 }
@@ -304,7 +322,7 @@ struct TdWarp {
 // A warp's winner buffer ran full: degree lookup and append of its entries
 // (all 32 lanes call).
 template <bool kDefer>
-__device__ __forceinline__ void flush_winners(const DobfsParams& p, TdWarp& tw, uint32_t& wcnt, uint32_t nxt,
+__device__ __forceinline__ void flush_winners(const DobfsParams& p, const StepView& sv, TdWarp& tw, uint32_t& wcnt,
                                               unsigned long long& scout, uint32_t& nbig) {
   const unsigned lane = threadIdx.x & 31;
   __syncwarp();
@@ -327,7 +345,7 @@ __device__ __forceinline__ void flush_winners(const DobfsParams& p, TdWarp& tw, 
       if (mask & (1u << k)) d[k] = p.off[v[k] + 1] - p.off[v[k]];
 #pragma unroll
     for (int k = 0; k < kVisit; ++k) scout += d[k];
-    append_warp<kVisit, kDefer>(p, nxt, v, d, mask, nbig);
+    append_warp<kVisit, kDefer>(p, sv, v, d, mask, nbig);
   }
   wcnt = 0;
   __syncwarp();
@@ -336,7 +354,7 @@ __device__ __forceinline__ void flush_winners(const DobfsParams& p, TdWarp& tw, 
 // End of a step: every warp's remaining buffered winners are appended with
 // one reservation for the whole block.  All threads of the block call.
 template <bool kDefer>
-__device__ __forceinline__ void flush_block(const DobfsParams& p, TdWarp* tws, uint32_t wcnt, uint32_t nxt,
+__device__ __forceinline__ void flush_block(const DobfsParams& p, const StepView& sv, TdWarp* tws, uint32_t wcnt,
                                             unsigned long long& scout, uint32_t& nbig, bool count_scout) {
   __shared__ uint32_t s_cnt[kWarps];
   if ((threadIdx.x & 31) == 0) s_cnt[threadIdx.x >> 5] = wcnt;
@@ -360,7 +378,7 @@ __device__ __forceinline__ void flush_block(const DobfsParams& p, TdWarp* tws, u
 #pragma unroll
     for (int w = 0; w < kWarps; ++w) scout += d[w];
   }
-  append_block<kWarps, kDefer>(p, nxt, v, d, mask, nbig);
+  append_block<kWarps, kDefer>(p, sv, v, d, mask, nbig);
 }
 
 // One batch of top-down edge tests (bfs.hpp:280-289): lane edges u[k] -> v[k]
@@ -371,9 +389,10 @@ __device__ __forceinline__ void flush_block(const DobfsParams& p, TdWarp* tws, u
 // winner) and is buffered; scout and the next queue are updated when the
 // buffer is flushed.  All 32 lanes must call.
 template <bool kDefer>
-__device__ __forceinline__ void visit_batch(const DobfsParams& p, uint32_t* __restrict__ parents, uint32_t nxt,
-                                            const uint32_t (&u)[kVisit], const uint32_t (&v)[kVisit], uint32_t valid,
-                                            TdWarp& tw, uint32_t& wcnt, unsigned long long& scout, uint32_t& nbig) {
+__device__ __forceinline__ void visit_batch(const DobfsParams& p, const StepView& sv, const uint32_t (&u)[kVisit],
+                                            const uint32_t (&v)[kVisit], uint32_t valid, TdWarp& tw, uint32_t& wcnt,
+                                            unsigned long long& scout, uint32_t& nbig) {
+  uint32_t* __restrict__ parents = sv.parents;
   uint32_t w[kVisit];
 #pragma unroll
   for (int k = 0; k < kVisit; ++k) w[k] = (valid & (1u << k)) ? p.V[v[k] >> 5] : ~0u;
@@ -405,7 +424,7 @@ __device__ __forceinline__ void visit_batch(const DobfsParams& p, uint32_t* __re
     }
   }
   wcnt += tot;
-  if (wcnt > kWinBuf - 32 * kVisit) flush_winners<kDefer>(p, tw, wcnt, nxt, scout, nbig);
+  if (wcnt > kWinBuf - 32 * kVisit) flush_winners<kDefer>(p, sv, tw, wcnt, scout, nbig);
 }
 
 // Largest range index whose exclusive prefix (in `excl`) is <= e.
@@ -425,9 +444,9 @@ __device__ __forceinline__ int owner_of(const uint32_t* excl, uint32_t e) {
 // out as scalar edges, kVisit per lane per batch.  A unit's range is found by
 // binary search over the prefix in shared memory.  All 32 lanes must call.
 template <bool kDefer>
-__device__ __forceinline__ void gather_ranges(const DobfsParams& p, uint32_t* __restrict__ parents, uint32_t nxt,
-                                              uint32_t u, uint64_t lo, uint64_t hi, TdWarp& tw, uint32_t& wcnt,
-                                              unsigned long long& scout, uint32_t& nbig) {
+__device__ __forceinline__ void gather_ranges(const DobfsParams& p, const StepView& sv, uint32_t u, uint64_t lo,
+                                              uint64_t hi, TdWarp& tw, uint32_t& wcnt, unsigned long long& scout,
+                                              uint32_t& nbig) {
   const unsigned lane = threadIdx.x & 31;
   const uint64_t al   = min(hi, (lo + 3) & ~(uint64_t)3);
   const uint64_t ah   = max(al, hi & ~(uint64_t)3);
@@ -464,7 +483,7 @@ __device__ __forceinline__ void gather_ranges(const DobfsParams& p, uint32_t* __
       vv[3] = x.w;
       valid = 0xFu;
     }
-    visit_batch<kDefer>(p, parents, nxt, uu, vv, valid, tw, wcnt, scout, nbig);
+    visit_batch<kDefer>(p, sv, uu, vv, valid, tw, wcnt, scout, nbig);
   }
   for (uint32_t j = 0; j < stot; j += 32 * kVisit) {
     uint32_t uu[kVisit], vv[kVisit], valid = 0;
@@ -482,7 +501,7 @@ __device__ __forceinline__ void gather_ranges(const DobfsParams& p, uint32_t* __
         valid |= 1u << k;
       }
     }
-    visit_batch<kDefer>(p, parents, nxt, uu, vv, valid, tw, wcnt, scout, nbig);
+    visit_batch<kDefer>(p, sv, uu, vv, valid, tw, wcnt, scout, nbig);
   }
   __syncwarp();
 }
@@ -490,8 +509,11 @@ __device__ __forceinline__ void gather_ranges(const DobfsParams& p, uint32_t* __
 // ---------------------------------------------------------------------------
 // k_init: parents := null except root (bfs.hpp:175,180), V := {root},
 // control block := the reference's initial state (bfs.hpp:166-181).
+// reset_barrier: clear the grid barrier's arrival count (not in a kernel
+// whose blocks may already be waiting at that barrier).
 __device__ __forceinline__ void init_step(const DobfsParams& p, uint32_t root, uint32_t alpha, uint32_t beta,
-                                          uint32_t* parents, uint32_t topdown_only, uint32_t block, uint32_t nblocks) {
+                                          uint32_t* parents, uint32_t topdown_only, uint32_t block, uint32_t nblocks,
+                                          bool reset_barrier = true) {
   const uint64_t n      = p.n;
   const uint64_t tid    = (uint64_t)block * blockDim.x + threadIdx.x;
   const uint64_t stride = (uint64_t)nblocks * blockDim.x;
@@ -561,9 +583,10 @@ __device__ __forceinline__ void init_step(const DobfsParams& p, uint32_t root, u
     c.status      = 0;
     c.pre_decided = 0;
     c.bu_push     = 0;
-    p.ctrl->bar.count = 0;
+    if (reset_barrier) p.ctrl->bar.count = 0;
     p.ctrl->err       = 0;
     p.ctrl->decides   = 0;
+    p.ctrl->kernels   = 0;
     c.reached     = 1;
     c.t_start     = globaltimer();
     c.trace_len = 0;
@@ -581,13 +604,17 @@ __device__ __forceinline__ uint64_t frontier_size(const CtrlHdr& c, uint32_t qi)
   return (c.qpos[qi] & 0xFFFFFFFFull) + c.qbig[qi];
 }
 
+// Appends one trace record.  Only the writer (the one thread that owns the
+// trace) stores it; every copy of the state counts it, so copies stay equal.
 __device__ __forceinline__ void trace_add(Ctrl* ctrl, CtrlHdr& c, uint8_t dir, uint64_t frontier, uint64_t found,
-                                          unsigned long long now) {
+                                          unsigned long long now, bool writer) {
   if (c.trace_len < NWG_TRACE_CAP) {
-    ctrl->trace_dir[c.trace_len]      = dir;
-    ctrl->trace_frontier[c.trace_len] = frontier;
-    ctrl->trace_found[c.trace_len]    = found;
-    ctrl->trace_end_ns[c.trace_len]   = now - c.t_start;
+    if (writer) {
+      ctrl->trace_dir[c.trace_len]      = dir;
+      ctrl->trace_frontier[c.trace_len] = frontier;
+      ctrl->trace_found[c.trace_len]    = found;
+      ctrl->trace_end_ns[c.trace_len]   = now - c.t_start;
+    }
     c.trace_len++;
   }
 }
@@ -616,44 +643,53 @@ __device__ __forceinline__ uint32_t td_kernel_setup(CtrlHdr& c) {
 // front are exactly the unvisited out-neighbours of the front, so the step
 // discovers the same set and the same awake count as bfs.hpp:211-228; only
 // a parent may name another front vertex, which BFSVerifier's rules allow.
-// The push is taken when its estimated bytes are below the pull's: a pull
-// reads about 48 B per candidate (unvisited, with in-edges: offsets and the
-// first column sector); a push reads an offset sector per front vertex,
-// 4 B per front out-edge and about 50 B per discovery (degree, claim,
-// parent, queue entry), discoveries estimated as at most twice the front.
+// The push is taken when its estimated time is below the pull's, in tenths
+// of a nanosecond, with costs fitted to B200 step times of the RMAT,
+// uniform and grid workloads at 2^24 vertices:
+//   push: 300 per front vertex (queue entry, offsets), 50 per front
+//         out-edge (column, visited test), 500 per discovery (claim,
+//         parent, degree, queue entry);
+//   pull: 26 per vertex (the bitmap scan) plus, per candidate (unvisited,
+//         with in-edges), 30 per in-edge tested, growing with the scan
+//         length (x (1 + t / 16)), where an in-edge is in the front with
+//         probability about front_edges / m, so t = min(average degree,
+//         m / front_edges).
+// Discoveries are estimated as the front's out-edges times the unvisited
+// share, at most the candidates, and, on graphs of average degree <= 8
+// (meshes and roads, whose fronts are bands), at most twice the front.
 __device__ __forceinline__ bool pull_as_push(const DobfsParams& p, const CtrlHdr& c, uint64_t front,
                                              uint64_t front_edges) {
-  if (!p.symmetric) return false;
-  const uint64_t excl = p.nzero + c.reached;
-  const uint64_t cand = p.n > excl ? p.n - excl : 0;
-  const uint64_t wins = min(cand, 2 * front);
-  return 32 * front + 4 * front_edges + 50 * wins < 48 * cand;
+  if (!p.symmetric || front_edges == 0) return false;
+  const uint64_t excl   = p.nzero + c.reached;
+  const uint64_t cand   = p.n > excl ? p.n - excl : 0;
+  const uint64_t active = p.n > p.nzero ? p.n - p.nzero : 1;  // vertices with edges
+  const uint64_t avgdeg = max((uint64_t)1, p.m / active);
+  uint64_t       wins   = min(cand, (uint64_t)((double)front_edges * (double)cand / (double)active));
+  if (avgdeg <= 8) wins = min(wins, 2 * front);
+  const uint64_t t      = max((uint64_t)1, min(avgdeg, p.m / front_edges));
+  const uint64_t push   = 300 * front + 50 * front_edges + 500 * wins;
+  const uint64_t pull   = 26 * p.n + cand * (30 * t + 30 * t * t / 16);
+  return push < pull;
 }
 
 // ---------------------------------------------------------------------------
-// decide_core: one thread; consumes the previous action's counters and picks
-// the next action.  Every branch below cites the reference line it
-// reproduces.  The control header is loaded and stored with 16-byte vector
-// accesses so the decision costs one memory round trip, not one per field.
-// Returns the next action (kActNone when the traversal is over).
-__device__ uint32_t decide_core(const DobfsParams& p) {
+// decide_on: one thread; consumes the previous action's counters (already
+// in `c`) and picks the next action.  Every branch below cites the reference
+// line it reproduces.  Returns the next action (kActNone when the traversal
+// is over).  It advances a copy `c` of the decision state; `writer` marks
+// the one caller that writes the trace.  It reads nothing else that changes
+// during a step except the sticky error word, so equal copies given equal
+// counters make equal decisions.
+__device__ uint32_t decide_on(const DobfsParams& p, CtrlHdr& c, bool writer) {
   const unsigned long long now = globaltimer();
-  constexpr int            kV  = sizeof(CtrlHdr) / 16;
-  CtrlHdr                  c;
-  {
-    const uint4* src = reinterpret_cast<const uint4*>(&p.ctrl->h);
-    uint4*       dst = reinterpret_cast<uint4*>(&c);
-#pragma unroll
-    for (int i = 0; i < kV; ++i) dst[i] = __ldcg(src + i);
-  }
   const uint64_t N    = p.n;
   uint32_t       next = kActNone;
   bool           done = false, queue_decision = false;
 
   switch (c.action) {
     case kActNone:  // first iteration: frontier = {root}
-      queue_decision         = true;
-      p.ctrl->t_first_decide = now - c.t_start;
+      queue_decision = true;
+      if (writer) p.ctrl->t_first_decide = now - c.t_start;
       break;
     case kActTD:
     case kActTDSmall:
@@ -662,7 +698,7 @@ __device__ uint32_t decide_core(const DobfsParams& p) {
       const uint64_t nq  = frontier_size(c, nxt);
       if (c.bu_push) {  // a bottom-up pull run as a push: the pull's bookkeeping
         const uint64_t awake = nq;
-        trace_add(p.ctrl, c, 1, c.old_awake, awake, now);
+        trace_add(p.ctrl, c, 1, c.old_awake, awake, now, writer);
         c.bu_steps++;
         c.reached += awake;
         c.cur = nxt;  // the discoveries, held as a queue, are the next front
@@ -691,7 +727,7 @@ __device__ uint32_t decide_core(const DobfsParams& p) {
         }
         break;
       }
-      trace_add(p.ctrl, c, 0, frontier_size(c, c.cur), nq, now);
+      trace_add(p.ctrl, c, 0, frontier_size(c, c.cur), nq, now, writer);
       c.td_steps++;
       c.reached += nq;
       c.scout_count = c.acc_scout;  // bfs.hpp:271
@@ -706,7 +742,7 @@ __device__ uint32_t decide_core(const DobfsParams& p) {
     }
     case kActBU: {
       const uint64_t awake = c.acc_awake;
-      trace_add(p.ctrl, c, 1, c.old_awake, awake, now);
+      trace_add(p.ctrl, c, 1, c.old_awake, awake, now, writer);
       c.bu_steps++;
       c.reached += awake;
       c.bm ^= 1u;  // C[bm] now holds this pull's discoveries (the new "front")
@@ -760,17 +796,34 @@ __device__ uint32_t decide_core(const DobfsParams& p) {
   if (!done && ++c.steps > c.max_steps) {
     c.status = NWG_ETIMEDOUT;  // loop bound; a BFS needs at most ~2n actions
   }
-  if (c.status == 0 && *(volatile int32_t*)&p.ctrl->err != 0) c.status = p.ctrl->err;
+  const int32_t err = *(volatile int32_t*)&p.ctrl->err;
+  if (c.status == 0 && err != 0) c.status = err;
   if (c.status != 0) done = true;
   c.action      = done ? kActNone : next;
   c.pre_decided = 0;
+  return c.action;
+}
+
+// decide_core: the decision on the control header itself (one thread).
+// The header is loaded and stored with 16-byte vector accesses so the
+// decision costs one memory round trip, not one per field.
+__device__ uint32_t decide_core(const DobfsParams& p) {
+  constexpr int kV = sizeof(CtrlHdr) / 16;
+  CtrlHdr       c;
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(&p.ctrl->h);
+    uint4*       dst = reinterpret_cast<uint4*>(&c);
+#pragma unroll
+    for (int i = 0; i < kV; ++i) dst[i] = __ldcg(src + i);
+  }
+  const uint32_t next = decide_on(p, c, true);
   {
     const uint4* src = reinterpret_cast<const uint4*>(&c);
     uint4*       dst = reinterpret_cast<uint4*>(&p.ctrl->h);
 #pragma unroll
     for (int i = 0; i < kV; ++i) dst[i] = src[i];
   }
-  return c.action;
+  return next;
 }
 
 // k_decide: the level loop's decision node.  When the previous action (the
@@ -798,17 +851,12 @@ __global__ void k_decide(DobfsParams p) {
 // hubs spread over the grid), then the small-degree queue; both go through
 // gather_ranges, a group of entries per warp.  The group size of chunk
 // entries shrinks when there are few so every warp gets work.
-// Returns the queue buffer the step wrote (read before any barrier that lets
-// the decide kernel swap the buffers).
 template <bool kDefer>
-__device__ __forceinline__ uint32_t td_step(const DobfsParams& p, TdWarp* tws, uint32_t block, uint32_t nblocks) {
-  CtrlHdr*           c       = &p.ctrl->h;
-  const uint32_t     cur     = __ldcg(&c->cur);
-  const uint32_t     nxt     = cur ^ 1u;
-  uint32_t* const    parents = c->parents;
-  const uint64_t     qpos    = __ldcg(&c->qpos[cur]);
-  const uint64_t     nS      = min((uint64_t)(qpos & 0xFFFFFFFFull), p.qs_cap);
-  const uint64_t     nC      = min((uint64_t)(qpos >> 32), p.qc_cap);
+__device__ __forceinline__ void td_step(const DobfsParams& p, const StepView& sv, TdWarp* tws, uint32_t block,
+                                        uint32_t nblocks) {
+  const uint32_t     cur     = sv.in;
+  const uint64_t     nS      = sv.nS;
+  const uint64_t     nC      = sv.nC;
   TdWarp&            tw      = tws[threadIdx.x >> 5];
   uint32_t           nbig    = 0;
   const unsigned     lane    = threadIdx.x & 31;
@@ -831,7 +879,7 @@ __device__ __forceinline__ uint32_t td_step(const DobfsParams& p, TdWarp* tws, u
       lo = ob + (ent & 0xFFFFFFFFull) * p.th.chunk;
       hi = min(oe, lo + p.th.chunk);
     }
-    gather_ranges<kDefer>(p, parents, nxt, u, lo, hi, tw, wcnt, scout, nbig);
+    gather_ranges<kDefer>(p, sv, u, lo, hi, tw, wcnt, scout, nbig);
   }
 
   const uint32_t* qs = p.qs[cur];
@@ -844,24 +892,61 @@ __device__ __forceinline__ uint32_t td_step(const DobfsParams& p, TdWarp* tws, u
       lo = p.off[u];
       hi = p.off[u + 1];
     }
-    gather_ranges<kDefer>(p, parents, nxt, u, lo, hi, tw, wcnt, scout, nbig);
+    gather_ranges<kDefer>(p, sv, u, lo, hi, tw, wcnt, scout, nbig);
   }
-  flush_block<kDefer>(p, tws, wcnt, nxt, scout, nbig, true);
+  flush_block<kDefer>(p, sv, tws, wcnt, scout, nbig, true);
 
   const unsigned long long tot = block_sum(scout);
   __syncthreads();
   const uint32_t nb = block_sum(nbig);
   if (threadIdx.x == 0) {
-    if (tot) atomicAdd(&c->acc_scout, tot);
-    if (nb) atomicAdd(&c->qbig[nxt], nb);
+    if (tot) atomicAdd(sv.scout, tot);
+    if (nb) atomicAdd(sv.qbig, nb);
   }
-  return nxt;
+}
+
+// Views of the step the control header describes (the level-loop kernels).
+// A top-down step expands queue buffer cur into cur ^ 1.
+__device__ __forceinline__ StepView td_view(const DobfsParams& p) {
+  CtrlHdr*       c = &p.ctrl->h;
+  StepView       sv;
+  sv.parents       = c->parents;
+  sv.in            = __ldcg(&c->cur);
+  sv.out           = sv.in ^ 1u;
+  const uint64_t q = __ldcg(&c->qpos[sv.in]);
+  sv.nS            = min((uint64_t)(q & 0xFFFFFFFFull), p.qs_cap);
+  sv.nC            = min((uint64_t)(q >> 32), p.qc_cap);
+  sv.bu_mode       = 0;
+  sv.bm            = 0;
+  sv.qpos          = &c->qpos[sv.out];
+  sv.qbig          = &c->qbig[sv.out];
+  sv.nhub          = &c->nhub[sv.out];
+  sv.scout         = &c->acc_scout;
+  sv.awake         = &c->acc_awake;
+  return sv;
+}
+
+// A pull, or the bitmap -> queue pass that refills buffer cur.
+__device__ __forceinline__ StepView bu_view(const DobfsParams& p) {
+  CtrlHdr* c = &p.ctrl->h;
+  StepView sv;
+  sv.parents = c->parents;
+  sv.in = sv.out = __ldcg(&c->cur);
+  sv.nS = sv.nC = 0;
+  sv.bu_mode    = __ldcg(&c->bu_mode);
+  sv.bm         = __ldcg(&c->bm);
+  sv.qpos       = &c->qpos[sv.out];
+  sv.qbig       = &c->qbig[sv.out];
+  sv.nhub       = &c->nhub[sv.out];
+  sv.scout      = &c->acc_scout;
+  sv.awake      = &c->acc_awake;
+  return sv;
 }
 
 // k_td: one top-down step over the whole grid.
-__global__ void __launch_bounds__(kThreads, 3) k_td(DobfsParams p) {
+__global__ void __launch_bounds__(kThreads, kTdPerSm) k_td(DobfsParams p) {
   __shared__ TdWarp s_tw[kWarps];
-  td_step<false>(p, s_tw, blockIdx.x, gridDim.x);
+  td_step<false>(p, td_view(p), s_tw, blockIdx.x, gridDim.x);
 }
 
 // Grid-wide barrier of a cooperative launch.  The wait is bounded: after
@@ -918,10 +1003,11 @@ __device__ __forceinline__ bool grid_barrier(const DobfsParams& p, unsigned nblo
 // buffer qi): a warp per record, grid-strided, so the writes come from every
 // SM.  Runs after the level's barrier, beside the decision; the next barrier
 // (or the kernel's end) orders them before the next level reads the queue.
-__device__ __forceinline__ void expand_hubs(const DobfsParams& p, uint32_t qi, uint32_t block, uint32_t nblocks) {
+__device__ __forceinline__ void expand_hubs(const DobfsParams& p, uint32_t qi, uint64_t nhub, uint32_t block,
+                                            uint32_t nblocks) {
   const HubRec* rec = p.hubrec[qi];
   if (rec == nullptr) return;
-  const uint64_t  nrec   = min((uint64_t)__ldcg(&p.ctrl->h.nhub[qi]), p.hub_cap);
+  const uint64_t  nrec   = min(nhub, p.hub_cap);
   const unsigned  lane   = threadIdx.x & 31;
   const uint64_t  gwarp  = (uint64_t)block * kWarps + (threadIdx.x >> 5);
   const uint64_t  nwarps = (uint64_t)nblocks * kWarps;
@@ -940,9 +1026,10 @@ __global__ void __launch_bounds__(kThreads) k_td_loop(DobfsParams p) {
   __shared__ TdWarp   s_tw[kWarps];
   __shared__ uint32_t s_next;
   for (;;) {
-    const uint32_t wrote = td_step<true>(p, s_tw, blockIdx.x, gridDim.x);
+    const StepView sv = td_view(p);
+    td_step<true>(p, sv, s_tw, blockIdx.x, gridDim.x);
     if (!grid_barrier(p, gridDim.x)) break;
-    expand_hubs(p, wrote, blockIdx.x, gridDim.x);
+    expand_hubs(p, sv.out, __ldcg(sv.nhub), blockIdx.x, gridDim.x);
     if (blockIdx.x == 0 && threadIdx.x == 0) s_next = decide_core(p);
     if (!grid_barrier(p, gridDim.x)) break;
     if (threadIdx.x == 0) s_next = __ldcg(&p.ctrl->h.action);
@@ -978,9 +1065,10 @@ __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kThreads)
   const uint32_t    nblk    = cluster.num_blocks();
   uint32_t* const   rank0_next = cluster.map_shared_rank(&s_next, 0);  // rank 0's copy, read over DSMEM
   for (;;) {
-    const uint32_t wrote = td_step<true>(p, s_tw, rank, nblk);
+    const StepView sv = td_view(p);
+    td_step<true>(p, sv, s_tw, rank, nblk);
     cluster.sync();
-    expand_hubs(p, wrote, rank, nblk);
+    expand_hubs(p, sv.out, __ldcg(sv.nhub), rank, nblk);
     if (rank == 0 && threadIdx.x == 0) s_next = decide_core(p);
     cluster.sync();
     // every block reads the one decision rank 0 made; rank 0 writes it again
@@ -1037,13 +1125,12 @@ __device__ __forceinline__ uint32_t compact_tile(uint32_t bits, uint16_t* list) 
 // in-edges without a hit hands the rest of its list to the whole warp, 32
 // in-edges per step.  The first hit in row order becomes the parent, exactly
 // as the reference's sequential scan with `break`.
-__device__ __forceinline__ void bu_step(const DobfsParams& p, uint32_t block, uint32_t nblocks) {
+__device__ __forceinline__ void bu_step(const DobfsParams& p, const StepView& sv, uint32_t block, uint32_t nblocks) {
   __shared__ uint16_t s_cand[kWarps][kBuTileWords * 32];
   __shared__ uint32_t s_new[kWarps][kBuTileWords];
-  CtrlHdr*        c       = &p.ctrl->h;
-  const uint32_t  mode    = c->bu_mode;
-  const uint32_t  bm      = c->bm;
-  uint32_t* const parents = c->parents;
+  const uint32_t  mode    = sv.bu_mode;
+  const uint32_t  bm      = sv.bm;
+  uint32_t* const parents = sv.parents;
   const uint32_t* Cf      = bm ? p.C1 : p.C0;  // previous pull's discoveries
   uint32_t*       Cw      = bm ? p.C0 : p.C1;  // this pull's discoveries
   const uint32_t* front   = mode ? Cf : p.V;
@@ -1181,20 +1268,19 @@ __device__ __forceinline__ void bu_step(const DobfsParams& p, uint32_t block, ui
     __syncwarp();
   }
   const uint32_t tot = block_sum(awake);
-  if (threadIdx.x == 0 && tot) atomicAdd(&c->acc_awake, (unsigned long long)tot);
+  if (threadIdx.x == 0 && tot) atomicAdd(sv.awake, (unsigned long long)tot);
 }
 
-__global__ void __launch_bounds__(kThreads) k_bu(DobfsParams p) { bu_step(p, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(kThreads) k_bu(DobfsParams p) { bu_step(p, bu_view(p), blockIdx.x, gridDim.x); }
 
 // ---------------------------------------------------------------------------
 // k_b2q: bitmap -> queue (bfs.hpp:235-239) from C[bm], folding C[bm] into V
 // on the way.  Each warp compacts tiles of 32 words into its vertex buffer;
 // full buffers are appended per warp, the rest once per block at the end.
-__device__ __forceinline__ void b2q_step(const DobfsParams& p, TdWarp* s_tw, uint32_t block, uint32_t nblocks) {
+__device__ __forceinline__ void b2q_step(const DobfsParams& p, const StepView& sv, TdWarp* s_tw, uint32_t block,
+                                         uint32_t nblocks) {
   __shared__ uint16_t s_list[kWarps][kTileWords * 32];
-  CtrlHdr*           c      = &p.ctrl->h;
-  const uint32_t*    Cs     = c->bm ? p.C1 : p.C0;
-  const uint32_t     qi     = c->cur;
+  const uint32_t*    Cs     = sv.bm ? p.C1 : p.C0;
   const unsigned     lane   = threadIdx.x & 31;
   const unsigned     wib    = threadIdx.x >> 5;
   const uint64_t     gwarp  = (uint64_t)block * kWarps + wib;
@@ -1212,20 +1298,161 @@ __device__ __forceinline__ void b2q_step(const DobfsParams& p, TdWarp* s_tw, uin
     const uint64_t vbase = t * kTileWords * 32;
     for (uint32_t j = 0; j < total; j += 32) {
       const uint32_t k = min(32u, total - j);  // warp-uniform
-      if (wcnt + k > kWinBuf) flush_winners<false>(p, tw, wcnt, qi, scout, nbig);
+      if (wcnt + k > kWinBuf) flush_winners<false>(p, sv, tw, wcnt, scout, nbig);
       if (lane < k) tw.win[wcnt + lane] = (uint32_t)(vbase + list[j + lane]);
       wcnt += k;
     }
     __syncwarp();
   }
-  flush_block<false>(p, s_tw, wcnt, qi, scout, nbig, false);
+  flush_block<false>(p, sv, s_tw, wcnt, scout, nbig, false);
   const uint32_t nb = block_sum(nbig);
-  if (threadIdx.x == 0 && nb) atomicAdd(&c->qbig[qi], nb);
+  if (threadIdx.x == 0 && nb) atomicAdd(sv.qbig, nb);
 }
 
 __global__ void __launch_bounds__(kThreads) k_b2q(DobfsParams p) {
   __shared__ TdWarp s_tw[kWarps];
-  b2q_step(p, s_tw, blockIdx.x, gridDim.x);
+  b2q_step(p, bu_view(p), s_tw, blockIdx.x, gridDim.x);
+}
+
+// ---------------------------------------------------------------------------
+// k_trav: the whole traversal in one cooperative launch (every block
+// resident), one grid barrier between steps instead of the level-loop
+// graph's decide kernel and conditional nodes, which cost about 13 us per
+// step on a B200 (decide 1.5 us, 5 us from its end to the next kernel's
+// first block, 6 us from a kernel's end to the next decide).
+//
+// Every block keeps its own copy of the decision state in shared memory and
+// runs decide_on on it after each barrier; all copies start equal and see
+// the same counters, so every block takes the same action and reaches the
+// same barriers.  A step adds its counts into StepAcc slot step % 3; block 0
+// clears slot (step + 1) % 3 during the step.  That slot was last read in
+// the decisions at the start of step - 1, which every block finished before
+// the barrier ending step - 1, and it is next written in step + 1, after the
+// barrier ending this step.  Deferred hub chunk entries are written by the
+// whole grid after the barrier and a second barrier orders them before the
+// next step reads the queue.  The steps are the level-loop kernels' own
+// (td_step, bu_step, b2q_step); the barrier's arrival count is cleared by
+// the host before the launch.
+constexpr int kTravPerSm = 4;  // 64 registers: the top-down step does not spill
+// Traversals run as k_trav; off, as the level-loop CUDA graph (k_init, then
+// WHILE{k_decide, SWITCH{k_td, k_bu, k_b2q, k_td_loop, k_td_cluster}}).
+constexpr bool kPersistentTraversal = true;
+
+// Grid barrier of k_trav: every block arrives (even after an error, so the
+// others are not left waiting); the wait is bounded like grid_barrier's.
+__device__ __forceinline__ bool trav_barrier(const DobfsParams& p, unsigned nblocks) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    GridBar*       bar = &p.ctrl->bar;
+    int            ok  = 1;
+    const unsigned g   = ld_acquire(&bar->gen);
+    __threadfence();
+    if (atomicAdd(&bar->count, 1u) == nblocks - 1) {
+      atomicExch(&bar->count, 0u);
+      __threadfence();
+      atomicAdd(&bar->gen, 1u);
+    } else {
+      unsigned spins = 0;
+      while (ld_acquire(&bar->gen) == g) {
+        if (++spins > kBarrierSpins) {
+          atomicCAS(&p.ctrl->err, 0, NWG_ETIMEDOUT);
+          ok = 0;
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+__global__ void __launch_bounds__(kThreads, kTravPerSm)
+    k_trav(DobfsParams p, uint32_t root, uint32_t alpha, uint32_t beta, uint32_t* parents, uint32_t topdown_only) {
+  __shared__ TdWarp   s_tw[kWarps];
+  __shared__ CtrlHdr  s_c;  // this block's copy of the decision state
+  __shared__ uint32_t s_next;
+  constexpr int       kV = sizeof(CtrlHdr) / 16;
+  init_step(p, root, alpha, beta, parents, topdown_only, blockIdx.x, gridDim.x, false);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    for (int i = 0; i < 3; ++i) p.ctrl->acc[i] = StepAcc{};
+    p.ctrl->kernels = 1;
+  }
+  bool ok = trav_barrier(p, gridDim.x);
+  if (ok && threadIdx.x == 0) {
+    const uint4* src = reinterpret_cast<const uint4*>(&p.ctrl->h);
+    uint4*       dst = reinterpret_cast<uint4*>(&s_c);
+#pragma unroll
+    for (int i = 0; i < kV; ++i) dst[i] = __ldcg(src + i);
+  }
+  uint32_t last = kActNone;
+  for (uint32_t step = 0; ok; ++step) {
+    if (threadIdx.x == 0) {
+      if (step > 0) {  // the previous step's counters, final after the barrier
+        const StepAcc* a = &p.ctrl->acc[(step - 1) % 3];
+        if (last != kActBU) {
+          const uint32_t ob = last == kActB2Q ? s_c.cur : (s_c.cur ^ 1u);  // the queue buffer it wrote
+          s_c.qpos[ob]      = __ldcg(&a->qpos);
+          s_c.qbig[ob]      = __ldcg(&a->qbig);
+          s_c.nhub[ob]      = __ldcg(&a->nhub);
+        }
+        s_c.acc_scout = __ldcg(&a->scout);
+        s_c.acc_awake = __ldcg(&a->awake);
+      }
+      s_next = decide_on(p, s_c, blockIdx.x == 0);
+    }
+    __syncthreads();
+    const uint32_t next = s_next;
+    if (next == kActNone) break;
+    StepAcc* a = &p.ctrl->acc[step % 3];
+    if (blockIdx.x == 0 && threadIdx.x == 0) p.ctrl->acc[(step + 1) % 3] = StepAcc{};
+    StepView sv;
+    sv.parents = s_c.parents;
+    sv.bu_mode = s_c.bu_mode;
+    sv.bm      = s_c.bm;
+    sv.qpos    = &a->qpos;
+    sv.qbig    = &a->qbig;
+    sv.nhub    = &a->nhub;
+    sv.scout   = &a->scout;
+    sv.awake   = &a->awake;
+    if (next == kActBU) {
+      sv.in = sv.out = s_c.cur;
+      sv.nS = sv.nC = 0;
+      bu_step(p, sv, blockIdx.x, gridDim.x);
+    } else if (next == kActB2Q) {
+      sv.in = sv.out = s_c.cur;
+      sv.nS = sv.nC = 0;
+      b2q_step(p, sv, s_tw, blockIdx.x, gridDim.x);
+    } else {  // a top-down step, or a pull run as a push
+      sv.in          = s_c.cur;
+      sv.out         = s_c.cur ^ 1u;
+      const uint64_t q = s_c.qpos[s_c.cur];
+      sv.nS          = min((uint64_t)(q & 0xFFFFFFFFull), p.qs_cap);
+      sv.nC          = min((uint64_t)(q >> 32), p.qc_cap);
+      td_step<true>(p, sv, s_tw, blockIdx.x, gridDim.x);
+    }
+    ok = trav_barrier(p, gridDim.x);
+    if (ok && next != kActBU && next != kActB2Q) {
+      const uint32_t nh = __ldcg(&a->nhub);  // the same in every block after the barrier
+      if (nh) {
+        expand_hubs(p, sv.out, nh, blockIdx.x, gridDim.x);
+        ok = trav_barrier(p, gridDim.x);
+      }
+    }
+    last = next;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const int32_t err = __ldcg(&p.ctrl->err);
+    if (s_c.status == 0 && err != 0) s_c.status = err;
+    s_c.action = kActNone;
+    const uint4* src = reinterpret_cast<const uint4*>(&s_c);
+    uint4*       dst = reinterpret_cast<uint4*>(&p.ctrl->h);
+#pragma unroll
+    for (int i = 0; i < kV; ++i) dst[i] = src[i];
+  }
 }
 
 // In-degree-zero bitmap; bits past n are set so they are never candidates.
@@ -1391,11 +1618,11 @@ __global__ void __launch_bounds__(kThreads) k_ragged(RaggedParams rp) {
       const uint32_t next = s_next;
       if (next == kActNone) break;
       if (next == kActBU) {
-        bu_step(p, 0, 1);
+        bu_step(p, bu_view(p), 0, 1);
       } else if (next == kActB2Q) {
-        b2q_step(p, s_tw, 0, 1);
+        b2q_step(p, bu_view(p), s_tw, 0, 1);
       } else {
-        td_step<false>(p, s_tw, 0, 1);
+        td_step<false>(p, td_view(p), s_tw, 0, 1);
       }
       __syncthreads();
     }
@@ -1580,7 +1807,9 @@ int ws_init(GraphDev* g, Workspace* ws) {
   P.nzero        = g->nzero;
   P.symmetric    = g->symmetric ? 1u : 0u;
   P.ctrl         = ws->ctrl;
-  return build_exec(ws);
+  // every block of the persistent kernel must be resident (cooperative launch)
+  ws->trav_grid = resident_grid(g->sm_count, k_trav, kTravPerSm);
+  return kPersistentTraversal ? NWG_OK : build_exec(ws);
 }
 
 void ws_free(Workspace* ws) {
@@ -1605,6 +1834,9 @@ void ws_free(Workspace* ws) {
   delete ws;
 }
 
+// A traversal on `stream`: the persistent traversal kernel (one cooperative
+// launch after clearing its barrier's arrival count), or with
+// kPersistentTraversal off the level-loop CUDA graph.
 int ws_launch(Workspace* ws, uint32_t root, int alpha, int beta, uint32_t* parents, cudaStream_t stream,
               bool topdown_only) {
   GraphDev* g = ws->g;
@@ -1613,6 +1845,12 @@ int ws_launch(Workspace* ws, uint32_t root, int alpha, int beta, uint32_t* paren
   uint32_t  r = root, a = (uint32_t)alpha, b = (uint32_t)beta, td = topdown_only ? 1u : 0u;
   uint32_t* par    = parents ? parents : ws->parents;
   void*     args[] = {&ws->params, &r, &a, &b, &par, &td};
+  if (kPersistentTraversal) {
+    NWG_CUDA_TRY(cudaMemsetAsync(&ws->ctrl->bar, 0, sizeof(GridBar), stream));
+    NWG_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_trav, dim3(ws->trav_grid), dim3(kThreads), args, 0, stream));
+    ws->ran = true;
+    return NWG_OK;
+  }
   cudaKernelNodeParams kp = {};
   kp.func                 = (void*)k_init;
   kp.gridDim              = dim3(grid_for(g, 8));
@@ -1683,8 +1921,9 @@ int zero_indegree_into(const uint64_t* in_off, uint64_t n, uint32_t* Z, int sm_c
 
 void fill_stats(const Ctrl& c, nwg_bfs_stats* s) {
   s->status    = c.h.status ? c.h.status : c.err;
-  // the init kernel, every decide, and one action after each decide but the last
-  s->kernel_launches = 2 * c.decides;
+  // the persistent traversal kernel alone; or the init kernel, every decide,
+  // and one action after each decide but the last
+  s->kernel_launches = c.kernels ? c.kernels : 2 * c.decides;
   s->steps     = c.h.steps;
   s->levels    = c.h.levels;
   s->td_steps  = c.h.td_steps;

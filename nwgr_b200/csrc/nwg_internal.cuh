@@ -86,9 +86,22 @@ struct GridBar {
   alignas(128) unsigned int gen;    // generation, polled with acquire loads (own line)
 };
 
+// Counters of one step of the persistent traversal kernel (k_trav), which
+// rotates three of them so that a slot is cleared only when no block can
+// still be reading it.
+struct alignas(64) StepAcc {
+  unsigned long long qpos;   // output queues' entries: small | chunk << 32
+  unsigned long long scout;  // out-degree sum of the vertices a top-down step discovers
+  unsigned long long awake;  // vertices a pull discovers
+  uint32_t           qbig;   // chunked vertices appended
+  uint32_t           nhub;   // deferred hub records appended
+};
+
 struct Ctrl {
   CtrlHdr            h;
   GridBar            bar;
+  StepAcc            acc[3];
+  uint32_t           kernels;  // kernel launches of the traversal when one persistent kernel ran it (else 0)
   int32_t            err;  // set with atomics by a device wait that ran out (never overwritten by the header copy)
   uint32_t           decides;  // k_decide launches of the traversal (each loop iteration launches one)
   uint8_t            trace_dir[NWG_TRACE_CAP];
@@ -153,6 +166,7 @@ struct Workspace {
   cudaGraph_t     template_graph = nullptr;  // kept alive: init_node belongs to it
   cudaGraphExec_t exec[1] = {nullptr};     // the level loop (direction-optimizing or top-down only)
   cudaGraphNode_t init_node[1] = {nullptr};
+  int             trav_grid = 0;     // blocks of the persistent traversal kernel (all resident)
   DobfsParams     params{};
   bool            ran = false;
   bool            timed = false;
