@@ -1,17 +1,23 @@
 // Direction-optimizing BFS on sm_100a: the device level loop.
 //
 // Restates nw::graph::bfs(out, in, root, num_bins, alpha, beta)
-// (include/nwgraph/algorithms/bfs.hpp:160-311 in NWGraph) as a CUDA graph:
+// (include/nwgraph/algorithms/bfs.hpp:160-311 in NWGraph) as one persistent
+// cooperative kernel, k_trav: init, then per step a decision and one action
+// (top-down step, bottom-up pull, or bitmap -> queue), with a grid barrier
+// between steps and no host round trip.
 //
-//   k_init ──► WHILE(h_loop) { k_decide ──► SWITCH(h_switch) { k_td | k_bu | k_b2q | k_td_loop | k_td_cluster } }
+// The decision (decide_on) reproduces the reference's integer switch rules
+// exactly (scout_count > edges_to_check / alpha selects bottom-up,
+// bfs.hpp:186; stay bottom-up while awake >= old_awake or awake > N / beta,
+// bfs.hpp:229; scout_count = 1 after a bottom-up phase, bfs.hpp:241; stop
+// when the next queue is empty, bfs.hpp:297-303, or a pull finds nothing,
+// bfs.hpp:231-233).
 //
-// k_decide is a one-thread kernel that reproduces the reference's integer
-// switch rules exactly (scout_count > edges_to_check / alpha selects
-// bottom-up, bfs.hpp:186; stay bottom-up while awake >= old_awake or
-// awake > N / beta, bfs.hpp:229; scout_count = 1 after a bottom-up phase,
-// bfs.hpp:241; stop when the next queue is empty, bfs.hpp:297-303, or a pull
-// finds nothing, bfs.hpp:231-233) and sets the graph's conditional handles,
-// so no level makes a host round trip.
+// The same steps also run as separate kernels driven from the host (k_init,
+// k_decide, k_td, k_bu, k_b2q, and k_td_loop / k_td_cluster for runs of
+// small top-down levels): the host-stepped traversal that profilers see
+// kernel by kernel and that the entry point without allocation uses; and
+// per block in k_ragged, one whole traversal per block.
 //
 // Device state (HBM):
 //   parents[n]   output; null = 0xFFFFFFFF
@@ -826,22 +832,16 @@ __device__ uint32_t decide_core(const DobfsParams& p) {
   return next;
 }
 
-// k_decide: the level loop's decision node.  When the previous action (the
-// persistent small-frontier kernel) already decided, it only applies that
-// decision to the graph's conditional handles.
+// k_decide: the host-stepped traversal's decision (one thread).  When the
+// previous action (a persistent small-frontier kernel) already decided, it
+// only clears that mark; the host reads the action from the header.
 __global__ void k_decide(DobfsParams p) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   p.ctrl->decides++;  // only this thread writes it
-  uint32_t next;
   if (__ldcg(&p.ctrl->h.pre_decided)) {
-    next                  = __ldcg(&p.ctrl->h.action);
     p.ctrl->h.pre_decided = 0;
   } else {
-    next = decide_core(p);
-  }
-  if (p.set_cond) {
-    cudaGraphSetConditional(p.h_switch, next);
-    cudaGraphSetConditional(p.h_loop, next == kActNone ? 0u : 1u);
+    decide_core(p);
   }
 }
 
@@ -1334,9 +1334,6 @@ __global__ void __launch_bounds__(kThreads) k_b2q(DobfsParams p) {
 // (td_step, bu_step, b2q_step); the barrier's arrival count is cleared by
 // the host before the launch.
 constexpr int kTravPerSm = 4;  // 64 registers: the top-down step does not spill
-// Traversals run as k_trav; off, as the level-loop CUDA graph (k_init, then
-// WHILE{k_decide, SWITCH{k_td, k_bu, k_b2q, k_td_loop, k_td_cluster}}).
-constexpr bool kPersistentTraversal = true;
 
 // Grid barrier of k_trav: every block arrives (even after an error, so the
 // others are not left waiting); the wait is bounded like grid_barrier's.
@@ -1609,7 +1606,6 @@ __global__ void __launch_bounds__(kThreads) k_ragged(RaggedParams rp) {
     p.nzero                = 0;  // unknown here: the push-or-pull estimate then counts isolated vertices too
     p.symmetric            = 1;  // packed graphs are symmetric
     p.ctrl                 = reinterpret_cast<Ctrl*>(slot + L.ctrl);
-    p.set_cond             = 0;
     init_step(p, item.root, (uint32_t)item.alpha, (uint32_t)item.beta, rp.parents + item.out_base, 0u, 0, 1);
     __syncthreads();
     for (;;) {
@@ -1671,85 +1667,6 @@ int resident_grid(int sm_count, K kernel, int per_sm_cap) {
   return std::max(1, sm_count * std::min(per_sm, per_sm_cap));
 }
 
-// Builds the level-loop CUDA graph of a workspace.
-int build_exec(Workspace* ws) {
-  GraphDev*   g = ws->g;
-  cudaGraph_t graph;
-  NWG_CUDA_TRY(cudaGraphCreate(&graph, 0));
-  ws->template_graph = graph;
-  cudaGraphConditionalHandle h_loop, h_switch;
-  NWG_CUDA_TRY(cudaGraphConditionalHandleCreate(&h_loop, graph, 1, cudaGraphCondAssignDefault));
-
-  DobfsParams& P     = ws->params;
-  uint32_t     root0 = 0, alpha0 = 15, beta0 = 18, td0 = 0;
-  uint32_t*    par0  = ws->parents;
-  void*        init_args[] = {&P, &root0, &alpha0, &beta0, &par0, &td0};
-
-  cudaKernelNodeParams kp = {};
-  kp.func                 = (void*)k_init;
-  kp.gridDim              = dim3(resident_grid(g->sm_count, k_init, 8));
-  kp.blockDim             = dim3(kThreads);
-  kp.kernelParams         = init_args;
-  cudaGraphNode_t init_node;
-  NWG_CUDA_TRY(cudaGraphAddKernelNode(&init_node, graph, nullptr, 0, &kp));
-
-  cudaGraphNodeParams wp = {};
-  wp.type                = cudaGraphNodeTypeConditional;
-  wp.conditional.handle  = h_loop;
-  wp.conditional.type    = cudaGraphCondTypeWhile;
-  wp.conditional.size    = 1;
-  cudaGraphNode_t while_node;
-  NWG_CUDA_TRY(cudaGraphAddNode(&while_node, graph, &init_node, 1, &wp));
-  cudaGraph_t body = wp.conditional.phGraph_out[0];
-
-  NWG_CUDA_TRY(cudaGraphConditionalHandleCreate(&h_switch, body, kActNone, cudaGraphCondAssignDefault));
-  P.h_loop   = h_loop;
-  P.h_switch = h_switch;
-  P.set_cond = 1;
-
-  void*                decide_args[] = {&P};
-  cudaKernelNodeParams dp            = {};
-  dp.func                            = (void*)k_decide;
-  dp.gridDim                         = dim3(1);
-  dp.blockDim                        = dim3(32);
-  dp.kernelParams                    = decide_args;
-  cudaGraphNode_t decide_node;
-  NWG_CUDA_TRY(cudaGraphAddKernelNode(&decide_node, body, nullptr, 0, &dp));
-
-  cudaGraphNodeParams sp = {};
-  sp.type                = cudaGraphNodeTypeConditional;
-  sp.conditional.handle  = h_switch;
-  sp.conditional.type    = cudaGraphCondTypeSwitch;
-  sp.conditional.size    = kNumActions;
-  cudaGraphNode_t switch_node;
-  NWG_CUDA_TRY(cudaGraphAddNode(&switch_node, body, &decide_node, 1, &sp));
-
-  void*     kernels[kNumActions] = {(void*)k_td, (void*)k_bu, (void*)k_b2q, (void*)k_td_loop, (void*)k_td_cluster};
-  const int grids[kNumActions]   = {grid_for(g, kTdPerSm), resident_grid(g->sm_count, k_bu, 8),
-                                    resident_grid(g->sm_count, k_b2q, 8), kSmallBlocks, kClusterCtas};
-  for (int a = 0; a < kNumActions; ++a) {
-    void*                args[] = {&P};
-    cudaKernelNodeParams ap     = {};
-    ap.func                     = kernels[a];
-    ap.gridDim                  = dim3(grids[a]);
-    ap.blockDim                 = dim3(kThreads);
-    ap.kernelParams             = args;
-    cudaGraphNode_t n;
-    NWG_CUDA_TRY(cudaGraphAddKernelNode(&n, sp.conditional.phGraph_out[a], nullptr, 0, &ap));
-    if (a == kActTDSmall) {  // grid barriers need every block resident: cooperative launch
-      cudaLaunchAttributeValue v = {};
-      v.cooperative              = 1;
-      NWG_CUDA_TRY(cudaGraphKernelNodeSetAttribute(n, cudaLaunchAttributeCooperative, &v));
-    }
-  }
-
-  cudaGraphExec_t exec;
-  NWG_CUDA_TRY(cudaGraphInstantiate(&exec, graph, 0));
-  ws->exec[0]      = exec;
-  ws->init_node[0] = init_node;
-  return NWG_OK;
-}
-
 }  // namespace
 
 int ws_init(GraphDev* g, Workspace* ws) {
@@ -1809,7 +1726,7 @@ int ws_init(GraphDev* g, Workspace* ws) {
   P.ctrl         = ws->ctrl;
   // every block of the persistent kernel must be resident (cooperative launch)
   ws->trav_grid = resident_grid(g->sm_count, k_trav, kTravPerSm);
-  return kPersistentTraversal ? NWG_OK : build_exec(ws);
+  return NWG_OK;
 }
 
 void ws_free(Workspace* ws) {
@@ -1818,8 +1735,6 @@ void ws_free(Workspace* ws) {
   cudaGetDevice(&prev);
   cudaSetDevice(ws->device);
   if (ws->stream) cudaStreamSynchronize(ws->stream);
-  if (ws->exec[0]) cudaGraphExecDestroy(ws->exec[0]);
-  if (ws->template_graph) cudaGraphDestroy(ws->template_graph);
   if (ws->ev0) cudaEventDestroy(ws->ev0);
   if (ws->ev1) cudaEventDestroy(ws->ev1);
   if (ws->stream) cudaStreamDestroy(ws->stream);
@@ -1834,9 +1749,8 @@ void ws_free(Workspace* ws) {
   delete ws;
 }
 
-// A traversal on `stream`: the persistent traversal kernel (one cooperative
-// launch after clearing its barrier's arrival count), or with
-// kPersistentTraversal off the level-loop CUDA graph.
+// A traversal on `stream`: the persistent traversal kernel, one cooperative
+// launch after clearing its barrier's arrival count.
 int ws_launch(Workspace* ws, uint32_t root, int alpha, int beta, uint32_t* parents, cudaStream_t stream,
               bool topdown_only) {
   GraphDev* g = ws->g;
@@ -1845,19 +1759,8 @@ int ws_launch(Workspace* ws, uint32_t root, int alpha, int beta, uint32_t* paren
   uint32_t  r = root, a = (uint32_t)alpha, b = (uint32_t)beta, td = topdown_only ? 1u : 0u;
   uint32_t* par    = parents ? parents : ws->parents;
   void*     args[] = {&ws->params, &r, &a, &b, &par, &td};
-  if (kPersistentTraversal) {
-    NWG_CUDA_TRY(cudaMemsetAsync(&ws->ctrl->bar, 0, sizeof(GridBar), stream));
-    NWG_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_trav, dim3(ws->trav_grid), dim3(kThreads), args, 0, stream));
-    ws->ran = true;
-    return NWG_OK;
-  }
-  cudaKernelNodeParams kp = {};
-  kp.func                 = (void*)k_init;
-  kp.gridDim              = dim3(grid_for(g, 8));
-  kp.blockDim             = dim3(kThreads);
-  kp.kernelParams         = args;
-  NWG_CUDA_TRY(cudaGraphExecKernelNodeSetParams(ws->exec[0], ws->init_node[0], &kp));
-  NWG_CUDA_TRY(cudaGraphLaunch(ws->exec[0], stream));
+  NWG_CUDA_TRY(cudaMemsetAsync(&ws->ctrl->bar, 0, sizeof(GridBar), stream));
+  NWG_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_trav, dim3(ws->trav_grid), dim3(kThreads), args, 0, stream));
   ws->ran = true;
   return NWG_OK;
 }
@@ -1868,7 +1771,6 @@ int ws_launch(Workspace* ws, uint32_t root, int alpha, int beta, uint32_t* paren
 int run_stepped(const DobfsParams& params, int sm_count, uint32_t root, int alpha, int beta, uint32_t* parents,
                 cudaStream_t stream) {
   DobfsParams P = params;
-  P.set_cond    = 0;
   const int g_init = resident_grid(sm_count, k_init, 8);
   const int g_bu   = resident_grid(sm_count, k_bu, 8);
   const int g_b2q  = resident_grid(sm_count, k_b2q, 8);

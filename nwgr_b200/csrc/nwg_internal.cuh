@@ -143,9 +143,6 @@ struct DobfsParams {
   uint64_t        nzero;      // vertices without in-edges (0 where unknown: only a cost estimate uses it)
   uint32_t        symmetric;  // the in-CSR is the out-CSR (a pull may then run as a push)
   Ctrl*           ctrl;
-  cudaGraphConditionalHandle h_loop;
-  cudaGraphConditionalHandle h_switch;
-  uint32_t                   set_cond;  // 0 when the kernels are launched one by one from the host
 };
 
 struct GraphDev;
@@ -163,9 +160,6 @@ struct Workspace {
   Ctrl*           ctrl_host = nullptr;  // pinned mirror for stats
   cudaStream_t    stream = nullptr;   // owned stream for the synchronous API
   cudaEvent_t     ev0 = nullptr, ev1 = nullptr;
-  cudaGraph_t     template_graph = nullptr;  // kept alive: init_node belongs to it
-  cudaGraphExec_t exec[1] = {nullptr};     // the level loop (direction-optimizing or top-down only)
-  cudaGraphNode_t init_node[1] = {nullptr};
   int             trav_grid = 0;     // blocks of the persistent traversal kernel (all resident)
   DobfsParams     params{};
   bool            ran = false;

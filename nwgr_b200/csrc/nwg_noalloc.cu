@@ -134,7 +134,6 @@ extern "C" __attribute__((visibility("default"))) int nwg_bfs_noalloc(const uint
     P.symmetric     = in_off ? 0u : 1u;
     P.nzero         = 0;  // not counted here (it would need a reduction and a read-back)
     P.ctrl          = reinterpret_cast<Ctrl*>(base + kNaOffCtrl);
-    P.set_cond      = 0;
 
     // Everything the traversal reads before writing is (re)initialised here
     // or by the init kernel: Z below, V and the control block by k_init; the
