@@ -53,7 +53,7 @@ constexpr int kThreads     = 256;
 constexpr int kWarps       = kThreads / 32;
 constexpr int kBuProbe     = 4;   // in-edges a lane tests per round (independent loads)
 constexpr int kBuLane      = 32;  // in-edges a lane scans alone before the warp helps
-constexpr int kTileWords   = 32;  // bitmap words per warp tile of the bitmap->queue pass (1024 vertices)
+constexpr int kTileWords   = 16;  // bitmap words per warp tile of the bitmap->queue pass (512 vertices)
 constexpr int kBuTileWords = 8;   // bitmap words per pull tile (256 vertices)
 constexpr int kSmallBlocks = 64;  // grid of the small-frontier top-down branch
 constexpr int kClusterCtas = 8;   // the tiny-frontier branch: one cluster of this many blocks
@@ -323,6 +323,23 @@ struct TdWarp {
   uint64_t al[32];     // first edge of the aligned body
   uint64_t ah[32];     // end of the aligned body (= start of the tail)
   uint32_t win[kWinBuf];
+};
+
+// Shared memory of the step functions in one block.  A top-down step uses
+// tw, bitmap -> queue uses tw and list, a pull uses PullSmem; a kernel that
+// runs more than one kind of step overlays the two (StepShared), since no
+// two steps run at once.
+struct TdSmem {
+  TdWarp   tw[kWarps];
+  uint16_t list[kWarps][kTileWords * 32];  // bitmap -> queue: one tile's set bits (local vertex indices)
+};
+struct PullSmem {
+  uint16_t cand[kWarps][kBuTileWords * 32];  // a tile's candidates (local vertex indices)
+  uint32_t fresh[kWarps][kBuTileWords];      // a tile's discoveries
+};
+union StepShared {
+  TdSmem   td;
+  PullSmem pull;
 };
 
 // A warp's winner buffer ran full: degree lookup and append of its entries
@@ -882,12 +899,17 @@ __device__ __forceinline__ void td_step(const DobfsParams& p, const StepView& sv
     gather_ranges<kDefer>(p, sv, u, lo, hi, tw, wcnt, scout, nbig);
   }
 
+  // small vertices per warp group: fewer when there are few, so that every
+  // warp gets work (a frontier of 40k degree-32 vertices in groups of 32
+  // left three quarters of a 4-block-per-SM grid idle)
+  uint64_t sgs = 32;
+  while (sgs > 4 && nS < nwarps * sgs * 2) sgs >>= 1;
   const uint32_t* qs = p.qs[cur];
-  for (uint64_t g0 = gwarp * 32; g0 < nS; g0 += nwarps * 32) {
+  for (uint64_t g0 = gwarp * sgs; g0 < nS; g0 += nwarps * sgs) {
     const uint64_t i  = g0 + lane;
     uint32_t       u  = 0;
     uint64_t       lo = 0, hi = 0;
-    if (i < nS) {
+    if (lane < sgs && i < nS) {
       u  = __ldcg(qs + i);
       lo = p.off[u];
       hi = p.off[u + 1];
@@ -1125,9 +1147,8 @@ __device__ __forceinline__ uint32_t compact_tile(uint32_t bits, uint16_t* list) 
 // in-edges without a hit hands the rest of its list to the whole warp, 32
 // in-edges per step.  The first hit in row order becomes the parent, exactly
 // as the reference's sequential scan with `break`.
-__device__ __forceinline__ void bu_step(const DobfsParams& p, const StepView& sv, uint32_t block, uint32_t nblocks) {
-  __shared__ uint16_t s_cand[kWarps][kBuTileWords * 32];
-  __shared__ uint32_t s_new[kWarps][kBuTileWords];
+__device__ __forceinline__ void bu_step(const DobfsParams& p, const StepView& sv, PullSmem& sm, uint32_t block,
+                                        uint32_t nblocks) {
   const uint32_t  mode    = sv.bu_mode;
   const uint32_t  bm      = sv.bm;
   uint32_t* const parents = sv.parents;
@@ -1136,8 +1157,8 @@ __device__ __forceinline__ void bu_step(const DobfsParams& p, const StepView& sv
   const uint32_t* front   = mode ? Cf : p.V;
   const unsigned  lane    = threadIdx.x & 31;
   const unsigned  wib     = threadIdx.x >> 5;
-  uint16_t* const cand    = s_cand[wib];
-  uint32_t* const fresh   = s_new[wib];
+  uint16_t* const cand    = sm.cand[wib];
+  uint32_t* const fresh   = sm.fresh[wib];
   const uint64_t  ntiles  = (p.nwords + kBuTileWords - 1) / kBuTileWords;
   const unsigned  lt_mask = (1u << lane) - 1u;
   uint32_t        awake   = 0;
@@ -1271,22 +1292,25 @@ __device__ __forceinline__ void bu_step(const DobfsParams& p, const StepView& sv
   if (threadIdx.x == 0 && tot) atomicAdd(sv.awake, (unsigned long long)tot);
 }
 
-__global__ void __launch_bounds__(kThreads) k_bu(DobfsParams p) { bu_step(p, bu_view(p), blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(kThreads) k_bu(DobfsParams p) {
+  __shared__ PullSmem sm;
+  bu_step(p, bu_view(p), sm, blockIdx.x, gridDim.x);
+}
 
 // ---------------------------------------------------------------------------
 // k_b2q: bitmap -> queue (bfs.hpp:235-239) from C[bm], folding C[bm] into V
 // on the way.  Each warp compacts tiles of 32 words into its vertex buffer;
 // full buffers are appended per warp, the rest once per block at the end.
-__device__ __forceinline__ void b2q_step(const DobfsParams& p, const StepView& sv, TdWarp* s_tw, uint32_t block,
+__device__ __forceinline__ void b2q_step(const DobfsParams& p, const StepView& sv, TdSmem& sm, uint32_t block,
                                          uint32_t nblocks) {
-  __shared__ uint16_t s_list[kWarps][kTileWords * 32];
+  TdWarp* const      s_tw   = sm.tw;
   const uint32_t*    Cs     = sv.bm ? p.C1 : p.C0;
   const unsigned     lane   = threadIdx.x & 31;
   const unsigned     wib    = threadIdx.x >> 5;
   const uint64_t     gwarp  = (uint64_t)block * kWarps + wib;
   const uint64_t     nwarps = (uint64_t)nblocks * kWarps;
   const uint64_t     ntiles = (p.nwords + kTileWords - 1) / kTileWords;
-  uint16_t* const    list   = s_list[wib];
+  uint16_t* const    list   = sm.list[wib];
   TdWarp&            tw     = s_tw[wib];
   uint32_t           wcnt   = 0, nbig = 0;
   unsigned long long scout  = 0;
@@ -1310,8 +1334,8 @@ __device__ __forceinline__ void b2q_step(const DobfsParams& p, const StepView& s
 }
 
 __global__ void __launch_bounds__(kThreads) k_b2q(DobfsParams p) {
-  __shared__ TdWarp s_tw[kWarps];
-  b2q_step(p, bu_view(p), s_tw, blockIdx.x, gridDim.x);
+  __shared__ TdSmem sm;
+  b2q_step(p, bu_view(p), sm, blockIdx.x, gridDim.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -1369,9 +1393,9 @@ __device__ __forceinline__ bool trav_barrier(const DobfsParams& p, unsigned nblo
 
 __global__ void __launch_bounds__(kThreads, kTravPerSm)
     k_trav(DobfsParams p, uint32_t root, uint32_t alpha, uint32_t beta, uint32_t* parents, uint32_t topdown_only) {
-  __shared__ TdWarp   s_tw[kWarps];
-  __shared__ CtrlHdr  s_c;  // this block's copy of the decision state
-  __shared__ uint32_t s_next;
+  __shared__ StepShared sm;
+  __shared__ CtrlHdr    s_c;  // this block's copy of the decision state
+  __shared__ uint32_t   s_next;
   constexpr int       kV = sizeof(CtrlHdr) / 16;
   init_step(p, root, alpha, beta, parents, topdown_only, blockIdx.x, gridDim.x, false);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -1418,18 +1442,18 @@ __global__ void __launch_bounds__(kThreads, kTravPerSm)
     if (next == kActBU) {
       sv.in = sv.out = s_c.cur;
       sv.nS = sv.nC = 0;
-      bu_step(p, sv, blockIdx.x, gridDim.x);
+      bu_step(p, sv, sm.pull, blockIdx.x, gridDim.x);
     } else if (next == kActB2Q) {
       sv.in = sv.out = s_c.cur;
       sv.nS = sv.nC = 0;
-      b2q_step(p, sv, s_tw, blockIdx.x, gridDim.x);
+      b2q_step(p, sv, sm.td, blockIdx.x, gridDim.x);
     } else {  // a top-down step, or a pull run as a push
       sv.in          = s_c.cur;
       sv.out         = s_c.cur ^ 1u;
       const uint64_t q = s_c.qpos[s_c.cur];
       sv.nS          = min((uint64_t)(q & 0xFFFFFFFFull), p.qs_cap);
       sv.nC          = min((uint64_t)(q >> 32), p.qc_cap);
-      td_step<true>(p, sv, s_tw, blockIdx.x, gridDim.x);
+      td_step<true>(p, sv, sm.td.tw, blockIdx.x, gridDim.x);
     }
     ok = trav_barrier(p, gridDim.x);
     if (ok && next != kActBU && next != kActB2Q) {
@@ -1569,8 +1593,8 @@ __host__ __device__ inline SlotLayout slot_layout(uint64_t nmax, uint64_t mmax) 
 }
 
 __global__ void __launch_bounds__(kThreads) k_ragged(RaggedParams rp) {
-  __shared__ TdWarp   s_tw[kWarps];
-  __shared__ uint32_t s_item, s_next;
+  __shared__ StepShared sm;
+  __shared__ uint32_t   s_item, s_next;
   const SlotLayout    L    = slot_layout(rp.nmax, rp.mmax);
   unsigned char*      slot = rp.scratch + (uint64_t)blockIdx.x * rp.slot_bytes;
   for (;;) {
@@ -1614,11 +1638,11 @@ __global__ void __launch_bounds__(kThreads) k_ragged(RaggedParams rp) {
       const uint32_t next = s_next;
       if (next == kActNone) break;
       if (next == kActBU) {
-        bu_step(p, bu_view(p), 0, 1);
+        bu_step(p, bu_view(p), sm.pull, 0, 1);
       } else if (next == kActB2Q) {
-        b2q_step(p, bu_view(p), s_tw, 0, 1);
+        b2q_step(p, bu_view(p), sm.td, 0, 1);
       } else {
-        td_step<false>(p, td_view(p), s_tw, 0, 1);
+        td_step<false>(p, td_view(p), sm.td.tw, 0, 1);
       }
       __syncthreads();
     }

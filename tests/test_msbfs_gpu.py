@@ -188,6 +188,8 @@ def test_msbfs_many_passes_in_flight(nwg, port):
         assert st.passes == 5 and np.array_equal(d.cpu().numpy(), want)
     d16 = torch.empty((roots.size, n), dtype=torch.int16, device="cuda")
     ws.run_ex(roots, d16)
-    assert np.array_equal(d16.cpu().numpy().view(np.uint16), np.where(want == 255, 0xFFFF, want).astype(np.uint16))
+    w16 = want.astype(np.uint16)
+    w16[want == 255] = 0xFFFF
+    assert np.array_equal(d16.cpu().numpy().view(np.uint16), w16)
     ws.close()
     g.release()
