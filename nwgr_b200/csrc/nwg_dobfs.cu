@@ -53,7 +53,7 @@ constexpr int kThreads     = 256;
 constexpr int kWarps       = kThreads / 32;
 constexpr int kBuProbe     = 4;   // in-edges a lane tests per round (independent loads)
 constexpr int kBuLane      = 32;  // in-edges a lane scans alone before the warp helps
-constexpr int kTileWords   = 16;  // bitmap words per warp tile of the bitmap->queue pass (512 vertices)
+constexpr int kTileWords   = 16;  // bitmap words per warp tile of the bitmap->queue pass (512 vertices; <= 32)
 constexpr int kBuTileWords = 8;   // bitmap words per pull tile (256 vertices)
 constexpr int kSmallBlocks = 64;  // grid of the small-frontier top-down branch
 constexpr int kClusterCtas = 8;   // the tiny-frontier branch: one cluster of this many blocks
@@ -1315,10 +1315,10 @@ __device__ __forceinline__ void b2q_step(const DobfsParams& p, const StepView& s
   uint32_t           wcnt   = 0, nbig = 0;
   unsigned long long scout  = 0;
   for (uint64_t t = gwarp; t < ntiles; t += nwarps) {
-    const uint64_t w = t * kTileWords + lane;
-    const uint32_t x = (w < p.nwords) ? Cs[w] : 0u;
+    const uint64_t w = t * kTileWords + lane;  // lanes >= kTileWords hold no word
+    const uint32_t x = (lane < kTileWords && w < p.nwords) ? Cs[w] : 0u;
     if (x) p.V[w] |= x;
-    const uint32_t total = compact_tile(x, list);
+    const uint32_t total = compact_tile(x, list);  // at most kTileWords * 32 entries
     const uint64_t vbase = t * kTileWords * 32;
     for (uint32_t j = 0; j < total; j += 32) {
       const uint32_t k = min(32u, total - j);  // warp-uniform

@@ -33,10 +33,13 @@ def _check(nwg, port, reference, off, cols, root, parents, stats, in_off=None, i
         g.close()
     if stats is not None:
         tr = stats.trace()
+        want_frontier = None
         if want_dir is None:
             _, ptr = port.dobfs(off, cols, int(root), in_off, in_cols)
-            want_dir, want_found = ptr["dir"], ptr["found"]
+            want_dir, want_found, want_frontier = ptr["dir"], ptr["found"], ptr["frontier"]
         k = min(len(want_dir), nwg.TRACE_CAP)
+        if want_frontier is not None:  # queue sizes entering top-down steps, previous awake counts entering pulls
+            assert np.array_equal(tr["frontier"][:k], np.asarray(want_frontier)[:k]), "per-step frontier sizes differ"
         assert stats.status == 0
         assert np.array_equal(tr["dir"][:k], np.asarray(want_dir)[:k]), "direction sequence differs"
         assert np.array_equal(tr["found"][:k], np.asarray(want_found)[:k]), "per-step discoveries differ"
