@@ -1361,7 +1361,8 @@ constexpr int kTravPerSm = 4;  // 64 registers: the top-down step does not spill
 
 // Grid barrier of k_trav: every block arrives (even after an error, so the
 // others are not left waiting); the wait is bounded like grid_barrier's.
-__device__ __forceinline__ bool trav_barrier(const DobfsParams& p, unsigned nblocks) {
+__device__ __forceinline__ bool trav_barrier(const DobfsParams& p, unsigned nblocks,
+                                             unsigned max_spins = kBarrierSpins) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -1376,7 +1377,7 @@ __device__ __forceinline__ bool trav_barrier(const DobfsParams& p, unsigned nblo
     } else {
       unsigned spins = 0;
       while (ld_acquire(&bar->gen) == g) {
-        if (++spins > kBarrierSpins) {
+        if (++spins > max_spins) {
           atomicCAS(&p.ctrl->err, 0, NWG_ETIMEDOUT);
           ok = 0;
           break;
@@ -2004,12 +2005,12 @@ int ragged_launch(RaggedDev* r, uint32_t n_items, uint32_t* parents_dev, uint32_
   return NWG_OK;
 }
 
-// Failure-detection probe: the persistent kernel's grid barrier, waited on
-// for one more block than the grid has, so no one ever releases it.  Every
-// block gives up after max_spins polls, records NWG_ETIMEDOUT and returns --
-// the path a real barrier takes when a block never arrives.
+// Failure-detection probe: the persistent traversal kernel's grid barrier,
+// waited on for one more block than the grid has, so no one ever releases
+// it.  Every block gives up after max_spins polls, records NWG_ETIMEDOUT and
+// returns -- the path a real barrier takes when a block never arrives.
 __global__ void k_wait_probe(DobfsParams p, unsigned max_spins) {
-  const bool ok = grid_barrier(p, gridDim.x + 1, max_spins);
+  const bool ok = trav_barrier(p, gridDim.x + 1, max_spins);
   if (!ok && threadIdx.x == 0 && blockIdx.x == 0) p.ctrl->h.status = __ldcg(&p.ctrl->err);
 }
 
