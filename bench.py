@@ -48,7 +48,8 @@ Further sections of the same JSON line (each skippable with --no-<name>):
   betweenness  brandes_bc over 64 sources on RMAT-22, beside the reference's
                on a 4-source sample
 Profiling modes (one run inside the NVTX range nwg_profile, for ncu):
---profile-one (single-source, host-stepped), --profile-msbfs, --profile-bc.
+--profile-one (single-source, host-stepped), --profile-trav (single-source,
+the persistent kernel), --profile-msbfs, --profile-bc.
 """
 from __future__ import annotations
 
@@ -71,11 +72,11 @@ GRAPH_SEED = 1
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum summed over the
-# kernels) of one traversal captured with ncu on a smaller graph of the same
-# kind, and that graph's directed entries; scaled to a workload by its
-# entries (profiles/dobfs_traffic_rmat22_uniform22.md).
-TRAFFIC_CAPTURES = {"rmat": (234.0e6, 128306546), "uniform": (542.8e6, 134217204)}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one traversal
+# (one launch of the persistent kernel k_trav) captured with ncu on a smaller
+# graph of the same kind, and that graph's directed entries; scaled to a
+# workload by its entries (profiles/k_trav_traffic_rmat22_uniform22.md).
+TRAFFIC_CAPTURES = {"rmat": (186.3e6, 128306546), "uniform": (532.7e6, 134217204)}
 
 
 def parse():
@@ -104,7 +105,11 @@ def parse():
                     help="betweenness from one source on RMAT-22 in NVTX range nwg_profile (for ncu)")
     ap.add_argument("--serve-slots", type=int, default=16)
     ap.add_argument("--profile-one", action="store_true",
-                    help="after warm-up, run one traversal inside an NVTX range 'nwg_profile' and exit (for ncu)")
+                    help="after warm-up, run one host-stepped traversal (one kernel per step) inside an NVTX range "
+                         "'nwg_profile' and exit (for ncu)")
+    ap.add_argument("--profile-trav", action="store_true",
+                    help="after warm-up, run one traversal as the persistent kernel k_trav inside an NVTX range "
+                         "'nwg_profile' and exit (for ncu)")
     return ap.parse_args()
 
 
@@ -293,7 +298,9 @@ def run_reference_arm(args, spec, world, rank):
         "vs_baseline": None, "dtype": "uint32", "data": "synthetic (seeded host generator)",
         "config": {"workload": workload_name(spec), "n": int(off.size - 1), "m_directed": int(cols.size),
                    "roots": int(roots.size), "alpha": 15, "beta": 18, "timing": "host wall clock per call"},
-        "cpu_baseline": {"value": v, "unit": "GTEPS", "cores": threads, "kind": "reference", "sample": sample},
+        "cpu_baseline": {"value": v, "unit": "GTEPS", "cores": threads, "kind": "reference",
+                         "ms_per_root_median": 1e3 * float(np.median(secs)),
+                         "glibc_tunables": os.environ.get("GLIBC_TUNABLES", ""), "sample": sample},
         "e2e": {"value": v, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -580,7 +587,7 @@ def bench_other_graphs(nwg, torch, main_graph, hbm, with_cpu, n_roots=16, reps=3
         if with_cpu:
             off, cols = g.csr()
             g.release()
-            row["cpu_reference"] = cpu_baseline(off, cols, roots, 4)
+            row["cpu_reference"] = cpu_baseline(off, cols, roots, 4, "after the device legs")
             del off, cols
         else:
             g.release()
@@ -588,7 +595,7 @@ def bench_other_graphs(nwg, torch, main_graph, hbm, with_cpu, n_roots=16, reps=3
     return out
 
 
-def cpu_baseline(off, cols, roots, n_roots):
+def cpu_baseline(off, cols, roots, n_roots, when="before the device legs"):
     """The reference's bfs.hpp on the host cores over the first n_roots roots
     (each once; all of them by default, the roots the reference arm times)."""
     from oracle.oracle import Reference
@@ -604,12 +611,40 @@ def cpu_baseline(off, cols, roots, n_roots):
     secs, edges = reference_roots_timed(rg, deg, roots, list(range(k)))
     rg.close()
     return {"value": hmean(edges / secs / 1e9), "unit": "GTEPS", "cores": ref.threads(), "kind": "reference",
+            "ms_per_root_median": 1e3 * float(np.median(secs)),
+            "glibc_tunables": os.environ.get("GLIBC_TUNABLES", ""),
             "sample": f"the first {k} of the {roots.size} roots, once each, reference bfs.hpp on the project's "
-                      f"TBB-compatible pool, wall clock around each call (time_op)"}
+                      f"TBB-compatible pool, wall clock around each call (time_op), {when}"}
+
+
+MALLOC_THP = "glibc.malloc.hugetlb=1"
+
+
+def reexec_with_malloc_thp(args):
+    """Restarts this process (same PID, arguments and environment) with
+    glibc's malloc asked to back its allocations with transparent huge
+    pages.  The reference's bfs allocates its parent array, bitmaps and
+    queues on every call; with 4 KB pages (THP in madvise mode, glibc's
+    default) the same calls ran 1.47x slower on RMAT-24.  Both CPU legs
+    (the reference arm and cpu_baseline) therefore run with it, the setting
+    under which the reference is fastest."""
+    if args.no_cpu and args.impl != "reference":
+        return
+    if args.profile_one or args.profile_trav or args.profile_msbfs or args.profile_bc:
+        return
+    cur = os.environ.get("GLIBC_TUNABLES", "")
+    if MALLOC_THP in cur.split(":"):
+        return
+    env = dict(os.environ)
+    env["GLIBC_TUNABLES"] = f"{cur}:{MALLOC_THP}" if cur else MALLOC_THP
+    sys.stdout.flush()
+    sys.stderr.flush()
+    os.execve(sys.executable, [sys.executable, os.path.abspath(__file__)] + sys.argv[1:], env)
 
 
 def main():
     args = parse()
+    reexec_with_malloc_thp(args)
     spec = graph_spec(args.graph)
     world, rank, local = dist_setup(args)
     import torch
@@ -636,6 +671,14 @@ def main():
     g = make_graph(nwg, spec)
     n, m = g.n, g.m
     roots = g.roots(args.roots, seed=ROOT_SEED)
+    # the reference on the host cores first, in the same process state as the
+    # reference arm (a fresh process holding only the graph): timed after the
+    # GPU legs, the same calls ran up to 40% faster or slower from run to run
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu and not (args.profile_one or args.profile_trav):
+        off, cols = g.csr()
+        cpu = cpu_baseline(off, cols, roots, args.cpu_sample_roots)
+        del off, cols
     stream = torch.cuda.Stream()
     ws = g.workspace()
     parents = torch.empty(n, dtype=torch.int32, device="cuda")
@@ -657,9 +700,22 @@ def main():
     e_r = np.asarray(e_r, np.float64)
     n_r = np.asarray(n_r, np.float64)
 
+    if args.profile_trav:
+        # one traversal = one launch of the persistent kernel, after an L2 flush
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+            torch.cuda.nvtx.range_push("nwg_profile")
+            ws.bfs_async(int(roots[0]), parents, stream.cuda_stream)
+            torch.cuda.nvtx.range_pop()
+        stream.synchronize()
+        st = ws.stats()
+        print(json.dumps({"profile_trav": True, "root": int(roots[0]), "n": n, "m": m, "steps": st.steps,
+                          "status": st.status, "kernel_launches": st.kernel_launches}))
+        return
+
     if args.profile_one:
-        # the same kernels launched one at a time from the host (ncu cannot
-        # profile kernels inside a CUDA graph with conditional nodes)
+        # the step kernels launched one at a time from the host (per-step
+        # figures; the persistent kernel runs all steps in one launch)
         nwg.bfs_stepped(g, int(roots[0]), parents)
         torch.cuda.synchronize()
         torch.cuda.nvtx.range_push("nwg_profile")
@@ -796,12 +852,6 @@ def main():
             g.release()
             ws, g = None, None
         bc = bench_bc(nwg, with_cpu=rank == 0 and not args.no_cpu)
-    cpu = None
-    if rank == 0 and not args.no_cpu:
-        if g is None:
-            g = make_graph(nwg, spec)
-        off, cols = g.csr()
-        cpu = cpu_baseline(off, cols, roots, args.cpu_sample_roots)
 
     if rank == 0:
         line = {

@@ -54,7 +54,7 @@ constexpr int kWarps       = kThreads / 32;
 constexpr int kBuProbe     = 4;   // in-edges a lane tests per round (independent loads)
 constexpr int kBuLane      = 32;  // in-edges a lane scans alone before the warp helps
 constexpr int kTileWords   = 16;  // bitmap words per warp tile of the bitmap->queue pass (512 vertices; <= 32)
-constexpr int kBuTileWords = 8;   // bitmap words per pull tile (256 vertices)
+constexpr int kBuTileWords = 16;  // bitmap words per pull tile (512 vertices; <= 32)
 constexpr int kSmallBlocks = 64;  // grid of the small-frontier top-down branch
 constexpr int kClusterCtas = 8;   // the tiny-frontier branch: one cluster of this many blocks
 constexpr int kClusterUnits = kClusterCtas * (kThreads / 32);  // its work-unit limit: one per warp
@@ -1128,12 +1128,16 @@ __device__ __forceinline__ uint32_t compact_tile(uint32_t bits, uint16_t* list) 
 // ---------------------------------------------------------------------------
 // k_bu: one bottom-up pull (bfs.hpp:211-228).
 //
-// Warps take tiles of kBuTileWords bitmap words (256 vertices), interleaved
+// Warps take tiles of kBuTileWords bitmap words (512 vertices), interleaved
 // over the grid (about seven tiles per warp at 2^24 vertices, so uneven tiles
-// average out).  A lane reads one word of V, of the previous pull's C and of
-// Z, folds C into V (the owner is the only writer), and the tile's
-// candidates (unvisited, with in-edges) are compacted into a per-warp list
-// in shared memory.
+// average out; 256-vertex tiles were 2-5% slower on RMAT and the grid).  A lane reads one word of V, of the previous pull's C and of
+// Z (loaded while the warp works on its previous tile), folds C into V (the
+// owner is the only writer), and the tile's candidates (unvisited, with
+// in-edges) are compacted into a per-warp list in shared memory.
+//
+// The front bitmap is read with plain (coherent) loads: in the persistent
+// traversal kernel it was written earlier in the same launch, by other SMs,
+// which the non-coherent path does not allow.
 //
 // The candidates then stream through the lanes.  Each lane holds the
 // candidate whose in-edges it is testing and the next one, whose in-CSR
@@ -1165,15 +1169,33 @@ __device__ __forceinline__ void bu_step(const DobfsParams& p, const StepView& sv
 
   const uint64_t  gwarp   = (uint64_t)block * kWarps + wib;
   const uint64_t  nwarps  = (uint64_t)nblocks * kWarps;
+  // V, C and Z words of the warp's next tile, loaded one tile ahead (the
+  // tiles are the warp's own, so no other warp writes these words)
+  uint32_t nxv = 0, nxf = 0, nxz = 0;
+  {
+    const uint64_t w = gwarp * kBuTileWords + lane;
+    if (gwarp < ntiles && lane < kBuTileWords && w < p.nwords) {
+      nxv = p.V[w];
+      nxf = mode ? Cf[w] : 0u;
+      nxz = p.Z[w];
+    }
+  }
   for (uint64_t t = gwarp; t < ntiles; t += nwarps) {
     const uint64_t w  = t * kBuTileWords + lane;
     const bool     wv = lane < kBuTileWords && w < p.nwords;
-    uint32_t       cm = 0;
+    const uint32_t vw = nxv, fw = nxf, zw = nxz;
+    {
+      const uint64_t wn = w + nwarps * kBuTileWords;
+      if (t + nwarps < ntiles && lane < kBuTileWords && wn < p.nwords) {
+        nxv = p.V[wn];
+        nxf = mode ? Cf[wn] : 0u;
+        nxz = p.Z[wn];
+      }
+    }
+    uint32_t cm = 0;
     if (wv) {
-      const uint32_t vw = p.V[w];
-      const uint32_t fw = mode ? Cf[w] : 0u;
       if (fw) p.V[w] = vw | fw;  // fold the previous pull into V
-      cm = ~(vw | fw) & ~p.Z[w];
+      cm = ~(vw | fw) & ~zw;
     }
     if (lane < kBuTileWords) fresh[lane] = 0;
     const uint32_t total = compact_tile(cm, cand);
@@ -1209,7 +1231,7 @@ __device__ __forceinline__ void bu_step(const DobfsParams& p, const StepView& sv
         uint32_t hit = 0;
 #pragma unroll
         for (int k = 0; k < kBuProbe; ++k)
-          if (nbv[k] != kNull && ((__ldg(front + (nbv[k] >> 5)) >> (nbv[k] & 31)) & 1u)) hit |= 1u << k;
+          if (nbv[k] != kNull && ((front[nbv[k] >> 5] >> (nbv[k] & 31)) & 1u)) hit |= 1u << k;
         if (hit) {
           const int k = __ffs(hit) - 1;
 #pragma unroll
@@ -1240,7 +1262,7 @@ __device__ __forceinline__ void bu_step(const DobfsParams& p, const StepView& sv
           bool           h = false;
           if (i < en) {
             v = __ldg(p.in_col + i);
-            h = (__ldg(front + (v >> 5)) >> (v & 31)) & 1u;
+            h = (front[v >> 5] >> (v & 31)) & 1u;
           }
           const unsigned hm = __ballot_sync(kFullMask, h);
           if (hm) {
@@ -1361,29 +1383,37 @@ constexpr int kTravPerSm = 4;  // 64 registers: the top-down step does not spill
 
 // Grid barrier of k_trav: every block arrives (even after an error, so the
 // others are not left waiting); the wait is bounded like grid_barrier's.
+// The arrival count only grows during a launch (the host clears it before
+// each one): the block that makes the k-th arrival waits until the count
+// reaches the next multiple of nblocks.  Passing costs one atomic per block
+// and the polls; there is no reset or generation word to update, so the
+// last block to arrive releases the others with its own arrival.  The fence
+// before the arrival and the acquire loads of the count order every
+// block's writes before the barrier ahead of every read after it.
+__device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long long* a) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(a) : "memory");
+  return v;
+}
+
 __device__ __forceinline__ bool trav_barrier(const DobfsParams& p, unsigned nblocks,
                                              unsigned max_spins = kBarrierSpins) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    GridBar*       bar = &p.ctrl->bar;
-    int            ok  = 1;
-    const unsigned g   = ld_acquire(&bar->gen);
+    unsigned long long* cnt = &p.ctrl->bar.arrivals;
+    int                 ok  = 1;
     __threadfence();
-    if (atomicAdd(&bar->count, 1u) == nblocks - 1) {
-      atomicExch(&bar->count, 0u);
-      __threadfence();
-      atomicAdd(&bar->gen, 1u);
-    } else {
-      unsigned spins = 0;
-      while (ld_acquire(&bar->gen) == g) {
-        if (++spins > max_spins) {
-          atomicCAS(&p.ctrl->err, 0, NWG_ETIMEDOUT);
-          ok = 0;
-          break;
-        }
-        __nanosleep(32);
+    const unsigned long long k      = atomicAdd(cnt, 1ull);
+    const unsigned long long target = (k / nblocks + 1) * nblocks;
+    unsigned                 spins  = 0;
+    while (ld_acquire64(cnt) < target) {
+      if (++spins > max_spins) {
+        atomicCAS(&p.ctrl->err, 0, NWG_ETIMEDOUT);
+        ok = 0;
+        break;
       }
+      __nanosleep(32);
     }
     __threadfence();
     s_ok = ok;

@@ -84,6 +84,9 @@ struct alignas(16) CtrlHdr {
 struct GridBar {
   alignas(128) unsigned int count;  // arrivals (own 128-byte line)
   alignas(128) unsigned int gen;    // generation, polled with acquire loads (own line)
+  // the persistent traversal kernel's barrier: arrivals since the launch,
+  // never reset inside it (barrier k is passed when it reaches k * blocks)
+  alignas(128) unsigned long long arrivals;
 };
 
 // Counters of one step of the persistent traversal kernel (k_trav), which
@@ -312,9 +315,10 @@ int      ms_ws_init_cap(GraphDev* g, uint64_t n_cap, uint64_t m_cap, MsWorkspace
 uint64_t ms_ws_bytes(uint64_t n_cap, uint64_t m_cap);
 void     ms_ws_free(MsWorkspace* ws);
 int      ms_run_on(MsWorkspace* ws, GraphDev* g, const uint32_t* roots_host, uint32_t k, void* depths_dev,
-                   uint32_t depth_bytes, uint8_t* deep_flags, int alpha, cudaStream_t stream, nwg_msbfs_stats* st);
+                   uint32_t depth_bytes, uint8_t* deep_flags, int alpha, cudaStream_t stream, nwg_msbfs_stats* st,
+                   cudaEvent_t end_ev = nullptr);
 int      ms_run(MsWorkspace* ws, const uint32_t* roots_host, uint32_t k, void* depths_dev, uint32_t depth_bytes,
-                uint8_t* deep_flags, int alpha, cudaStream_t stream, nwg_msbfs_stats* st);
+                uint8_t* deep_flags, int alpha, cudaStream_t stream, nwg_msbfs_stats* st, cudaEvent_t end_ev = nullptr);
 
 // nwg_gen.cu
 int gen_rmat(uint32_t scale, uint32_t ef, uint64_t seed, uint32_t ta, uint32_t tab, uint32_t tabc, GraphDev* g);

@@ -1120,8 +1120,13 @@ constexpr uint32_t kMsLanes = 4;  // passes of one call in flight at once
 // traversal on a workspace made for the purpose and freed again (such
 // sources are rare: a graph whose diameter passes 254); with uint8 rows it
 // keeps the depths up to 254 and 255 beyond.
+//
+// end_ev (may be null) is recorded on the stream once the call's device
+// work is enqueued, before the host waits for the last passes' records, so
+// that it marks the end of the device work rather than the host's wake-up.
 int ms_run_on(MsWorkspace* ws, GraphDev* g, const uint32_t* roots_host, uint32_t k, void* depths_dev,
-              uint32_t depth_bytes, uint8_t* deep_flags, int alpha, cudaStream_t stream, nwg_msbfs_stats* st) {
+              uint32_t depth_bytes, uint8_t* deep_flags, int alpha, cudaStream_t stream, nwg_msbfs_stats* st,
+              cudaEvent_t end_ev) {
   if (g->n > ws->n_cap || g->m > ws->m_cap)
     return set_error(NWG_EINVAL, "graph larger than the multi-source workspace's capacity");
   for (uint32_t i = 0; i < k; ++i)
@@ -1186,21 +1191,28 @@ int ms_run_on(MsWorkspace* ws, GraphDev* g, const uint32_t* roots_host, uint32_t
     const uint32_t kk = std::min<uint32_t>(256, k - 256 * p);
     rc = ms_launch_any(g, lane_ws(l), roots_host + 256 * p, kk, rows_of(p), depth_bytes, alpha, lane_stream(l));
   }
+  auto join = [&]() {  // `s` continues after every lane's work
+    for (uint32_t l = 1; l < nlanes; ++l) {
+      cudaEventRecord(ws->lanes[l - 1]->ev0, lane_stream(l));
+      cudaStreamWaitEvent(s, ws->lanes[l - 1]->ev0, 0);
+    }
+    if (end_ev) cudaEventRecord(end_ev, s);
+  };
+  join();
   while (done < npasses) {  // after an error, what was launched still completes before the call returns
     const int r = finish(done++);
     if (rc == NWG_OK) rc = r;
   }
-  for (uint32_t l = 1; l < nlanes; ++l) {  // `s` continues after every lane's work
-    cudaEventRecord(ws->lanes[l - 1]->ev0, lane_stream(l));
-    cudaStreamWaitEvent(s, ws->lanes[l - 1]->ev0, 0);
+  if (single) {  // uint16 rows of deep sources were computed after the passes
+    join();
+    ws_free(single);
   }
-  if (single) ws_free(single);
   return rc;
 }
 
 int ms_run(MsWorkspace* ws, const uint32_t* roots_host, uint32_t k, void* depths_dev, uint32_t depth_bytes,
-           uint8_t* deep_flags, int alpha, cudaStream_t stream, nwg_msbfs_stats* st) {
-  return ms_run_on(ws, ws->g, roots_host, k, depths_dev, depth_bytes, deep_flags, alpha, stream, st);
+           uint8_t* deep_flags, int alpha, cudaStream_t stream, nwg_msbfs_stats* st, cudaEvent_t end_ev) {
+  return ms_run_on(ws, ws->g, roots_host, k, depths_dev, depth_bytes, deep_flags, alpha, stream, st, end_ev);
 }
 
 }  // namespace nwg
