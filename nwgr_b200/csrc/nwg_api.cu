@@ -492,9 +492,9 @@ int msbfs_common(nwg_msbfs_ws h, const uint32_t* roots_host, uint32_t k, void* d
   DeviceGuard     dg(ws->g->device);
   nwg_msbfs_stats st = {};
   cudaStream_t    s  = stream ? reinterpret_cast<cudaStream_t>(stream) : ws->stream;
-  NWG_CUDA_TRY(cudaEventRecord(ws->ev0, s));
+  NWG_CUDA_TRY(cudaEventRecord(ws->ev0, s));  // re-recorded by ms_run before its first device operation
   NWG_CUDA_TRY(cudaEventRecord(ws->ev1, s));  // re-recorded by ms_run at the end of the device work
-  int rc = ms_run(ws, roots_host, k, depths_dev, depth_bytes, deep_flags, alpha, s, &st, ws->ev1);
+  int rc = ms_run(ws, roots_host, k, depths_dev, depth_bytes, deep_flags, alpha, s, &st, ws->ev1, ws->ev0);
   NWG_CUDA_TRY(cudaEventSynchronize(ws->ev1));
   cudaEventElapsedTime(&st.device_ms, ws->ev0, ws->ev1);
   st.status = rc;

@@ -60,6 +60,14 @@ constexpr int kClusterCtas = 8;   // the tiny-frontier branch: one cluster of th
 constexpr int kClusterUnits = kClusterCtas * (kThreads / 32);  // its work-unit limit: one per warp
 constexpr int kVisit       = 4;   // edges a lane claims per batch
 constexpr int kTdPerSm     = 4;   // k_td blocks per SM (64 registers per thread, no spills: 3% faster than 3 on the grid)
+// Solo levels of the persistent traversal kernel (block 0 alone): at most
+// this many frontier out-edges (so a level's discoveries fit a shared list;
+// one SM's loads and claims in flight bound it: a level of 2,000 edges took
+// 27 us alone against 15 us on the grid, one of 1,000 8 us), and at most
+// kSoloLevels levels per turn (the other blocks' wait).
+constexpr uint32_t kSoloCap    = 1024;
+constexpr uint32_t kSoloLevels = 256;
+constexpr uint32_t kSoloPer    = kSoloCap / kThreads;  // list entries per thread in the prefix pass
 
 __device__ __forceinline__ unsigned long long globaltimer() {
   unsigned long long t;
@@ -337,9 +345,18 @@ struct PullSmem {
   uint16_t cand[kWarps][kBuTileWords * 32];  // a tile's candidates (local vertex indices)
   uint32_t fresh[kWarps][kBuTileWords];      // a tile's discoveries
 };
+// Solo levels (k_trav, block 0 alone): the frontier and the next one as
+// vertex lists, and the exclusive prefix of the frontier's out-degrees.
+struct SoloSmem {
+  uint32_t q[2][kSoloCap];
+  uint32_t pre[kSoloCap + 1];
+  uint32_t cnt;
+  uint32_t nhub;
+};
 union StepShared {
   TdSmem   td;
   PullSmem pull;
+  SoloSmem solo;
 };
 
 // A warp's winner buffer ran full: degree lookup and append of its entries
@@ -613,6 +630,8 @@ __device__ __forceinline__ void init_step(const DobfsParams& p, uint32_t root, u
     c.reached     = 1;
     c.t_start     = globaltimer();
     c.trace_len = 0;
+    c.scout_exact = 1;  // scout_count = the root's out-degree
+    c.prev_small  = 0;
     const uint64_t cap = 2 * n + 64;
     c.max_steps = cap > 0xFFFFFF00ull ? 0xFFFFFF00u : (uint32_t)cap;
   }
@@ -703,12 +722,15 @@ __device__ __forceinline__ bool pull_as_push(const DobfsParams& p, const CtrlHdr
 // the one caller that writes the trace.  It reads nothing else that changes
 // during a step except the sticky error word, so equal copies given equal
 // counters make equal decisions.
-__device__ uint32_t decide_on(const DobfsParams& p, CtrlHdr& c, bool writer) {
+__device__ uint32_t decide_on(const DobfsParams& p, CtrlHdr& c, bool writer, bool read_err = true) {
   const unsigned long long now = globaltimer();
   const uint64_t N    = p.n;
   uint32_t       next = kActNone;
   bool           done = false, queue_decision = false;
 
+  const bool was_exact = c.scout_exact != 0;
+  if (c.action != kActNone) c.scout_exact = 0;  // set again below after a top-down step
+  c.prev_small = 0;
   switch (c.action) {
     case kActNone:  // first iteration: frontier = {root}
       queue_decision = true;
@@ -750,10 +772,12 @@ __device__ uint32_t decide_on(const DobfsParams& p, CtrlHdr& c, bool writer) {
         }
         break;
       }
+      c.prev_small = was_exact && c.scout_count <= kSoloCap && frontier_size(c, c.cur) <= kSoloCap;
       trace_add(p.ctrl, c, 0, frontier_size(c, c.cur), nq, now, writer);
       c.td_steps++;
       c.reached += nq;
       c.scout_count = c.acc_scout;  // bfs.hpp:271
+      c.scout_exact = 1;
       c.cur         = nxt;          // swap(q1, q2), bfs.hpp:304
       if (nq == 0) {
         done = true;  // all q2 bins empty, bfs.hpp:297-303
@@ -819,7 +843,7 @@ __device__ uint32_t decide_on(const DobfsParams& p, CtrlHdr& c, bool writer) {
   if (!done && ++c.steps > c.max_steps) {
     c.status = NWG_ETIMEDOUT;  // loop bound; a BFS needs at most ~2n actions
   }
-  const int32_t err = *(volatile int32_t*)&p.ctrl->err;
+  const int32_t err = read_err ? *(volatile int32_t*)&p.ctrl->err : 0;
   if (c.status == 0 && err != 0) c.status = err;
   if (c.status != 0) done = true;
   c.action      = done ? kActNone : next;
@@ -1397,7 +1421,7 @@ __device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long l
 }
 
 __device__ __forceinline__ bool trav_barrier(const DobfsParams& p, unsigned nblocks,
-                                             unsigned max_spins = kBarrierSpins) {
+                                             unsigned max_spins = kBarrierSpins, unsigned sleep_ns = 32) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -1413,13 +1437,263 @@ __device__ __forceinline__ bool trav_barrier(const DobfsParams& p, unsigned nblo
         ok = 0;
         break;
       }
-      __nanosleep(32);
+      __nanosleep(sleep_ns);
     }
     __threadfence();
     s_ok = ok;
   }
   __syncthreads();
   return s_ok != 0;
+}
+
+// ---------------------------------------------------------------------------
+// Solo levels.  A top-down step whose frontier has at most kSoloCap
+// out-edges moves a few thousand bytes; on the whole grid it still costs a
+// chain of global round trips (queue, offsets, columns, claims, degree
+// lookups, queue append, counters) plus a grid barrier and the decision,
+// 10-15 us.  Instead block 0 runs such levels alone, one after another,
+// with the frontier lists, the out-degree prefix and the counters in shared
+// memory, and the decision (decide_on, the same rules) made by its thread 0
+// after each level; the other blocks wait at one grid barrier.  When a
+// decision leaves the solo case (a bigger frontier, a pull, the level
+// bound, the end), block 0 writes the frontier into the global queue buffer
+// in the usual form (small entries, chunk entries of the vertices with
+// out-degree >= warp_min) and publishes its decision state, which the
+// other blocks adopt after the barrier.
+
+// Out-degree prefix of list[0, cnt) into pre (pre[cnt] = total); returns the
+// total.  Thread t takes entries [t * kSoloPer, (t + 1) * kSoloPer).  All
+// threads of the block call.
+__device__ __forceinline__ uint64_t solo_prefix(const DobfsParams& p, const uint32_t* list, uint32_t cnt,
+                                                uint32_t* pre) {
+  const uint32_t i0 = threadIdx.x * kSoloPer;
+  uint32_t       d[kSoloPer];
+  uint64_t       sum = 0;
+#pragma unroll
+  for (uint32_t k = 0; k < kSoloPer; ++k) {
+    d[k] = 0;
+    if (i0 + k < cnt) {
+      const uint32_t v = list[i0 + k];
+      d[k]             = (uint32_t)min(__ldg(p.off + v + 1) - __ldg(p.off + v), (uint64_t)0xFFFFFFFFu);
+      sum += d[k];
+    }
+  }
+  unsigned long long total = 0;
+  unsigned long long run   = block_excl_scan(sum, total);
+#pragma unroll
+  for (uint32_t k = 0; k < kSoloPer; ++k) {
+    if (i0 + k < cnt) pre[i0 + k] = (uint32_t)run;
+    run += d[k];
+  }
+  if (threadIdx.x == 0) pre[cnt] = (uint32_t)total;
+  __syncthreads();
+  return total;
+}
+
+// Largest index o in [0, cnt) with pre[o] <= e: the list entry whose edge
+// range holds flattened edge e (entries without edges share their
+// successor's prefix and are skipped).
+__device__ __forceinline__ uint32_t solo_owner(const uint32_t* pre, uint32_t cnt, uint32_t e) {
+  uint32_t lo = 0, hi = cnt - 1;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi + 1) >> 1;
+    if (pre[mid] <= e) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// One top-down level over list[0, cnt) (edges flattened, total E <=
+// kSoloCap): claims as in visit_batch (atomicOr on V; the winner writes the
+// parent), winners appended to out through the shared counter *ocnt.  A
+// thread takes kSoloBatch edges at once, phase by phase (owner searches,
+// then all offset loads, all column loads, all claims), so its loads are in
+// flight together; one chain per edge made a level of 2,000 edges take 25 us.
+// All threads of the block call.
+constexpr int kSoloBatch = (int)kSoloPer;
+__device__ __forceinline__ void solo_expand(const DobfsParams& p, uint32_t* parents, const uint32_t* list, uint32_t cnt,
+                                            const uint32_t* pre, uint32_t E, uint32_t* out, uint32_t* ocnt) {
+  for (uint32_t base = 0; base < E; base += kThreads * kSoloBatch) {
+    uint32_t u[kSoloBatch], v[kSoloBatch], r[kSoloBatch];
+    uint32_t valid = 0;
+#pragma unroll
+    for (int k = 0; k < kSoloBatch; ++k) {
+      const uint32_t e = base + k * kThreads + threadIdx.x;
+      u[k] = r[k] = 0;
+      if (e < E) {
+        const uint32_t o = solo_owner(pre, cnt, e);
+        u[k]             = list[o];
+        r[k]             = e - pre[o];  // the edge's rank in u's row
+        valid |= 1u << k;
+      }
+    }
+    uint64_t at[kSoloBatch];
+#pragma unroll
+    for (int k = 0; k < kSoloBatch; ++k) at[k] = (valid & (1u << k)) ? __ldg(p.off + u[k]) + r[k] : 0ull;
+#pragma unroll
+    for (int k = 0; k < kSoloBatch; ++k) v[k] = (valid & (1u << k)) ? __ldg(p.col + at[k]) : 0u;
+#pragma unroll
+    for (int k = 0; k < kSoloBatch; ++k)
+      r[k] = (valid & (1u << k)) ? atomicOr(p.V + (v[k] >> 5), 1u << (v[k] & 31)) : ~0u;
+#pragma unroll
+    for (int k = 0; k < kSoloBatch; ++k) {
+      if ((valid & (1u << k)) && !(r[k] & (1u << (v[k] & 31)))) {
+        parents[v[k]]       = u[k];
+        const uint32_t slot = atomicAdd(ocnt, 1u);  // winners <= E <= kSoloCap
+        if (slot < kSoloCap) out[slot] = v[k];
+      }
+    }
+  }
+}
+
+// Writes list[0, cnt) into queue buffer qi as the top-down kernels expect it
+// and records the buffer's counts in c.  A vertex with more than kLaneChunks
+// chunks gets a hub record instead (c.nhub[qi] of them), whose chunk entries
+// the whole grid writes before the next step, as after a top-down step; one
+// block writing a hub frontier's 10^5 entries took 100+ us.  Without record
+// buffers the block writes them: `spare` (kSoloCap words) lists those
+// entries' indices, sm.pre their first chunk slots.  All threads of the
+// block call.
+__device__ __forceinline__ void solo_publish(const DobfsParams& p, CtrlHdr& c, uint32_t qi, const uint32_t* list,
+                                             uint32_t cnt, uint32_t* spare, SoloSmem& sm) {
+  const uint32_t i0 = threadIdx.x * kSoloPer;
+  uint64_t       deg[kSoloPer];
+  uint32_t       ns = 0, nb = 0;
+  uint64_t       nch = 0;
+#pragma unroll
+  for (uint32_t k = 0; k < kSoloPer; ++k) {
+    deg[k] = 0;
+    if (i0 + k < cnt) {
+      const uint32_t v = list[i0 + k];
+      deg[k]           = __ldg(p.off + v + 1) - __ldg(p.off + v);
+      if (deg[k] < p.th.warp_min) {
+        ++ns;
+      } else {
+        nch += chunks_of(deg[k], p.th);
+        ++nb;
+      }
+    }
+  }
+  if (threadIdx.x == 0) sm.nhub = 0;
+  unsigned long long tot  = 0;
+  const unsigned long long excl = block_excl_scan((unsigned long long)ns | ((unsigned long long)nch << 32), tot);
+  const unsigned long long tb   = block_sum((unsigned long long)nb);
+  uint64_t spos = excl & 0xFFFFFFFFull, cpos = excl >> 32;
+  bool     over = false;
+  uint32_t* const qs = p.qs[qi];
+  uint64_t* const qc = p.qc[qi];
+#pragma unroll
+  for (uint32_t k = 0; k < kSoloPer; ++k) {
+    if (i0 + k >= cnt) continue;
+    const uint32_t v = list[i0 + k];
+    if (deg[k] < p.th.warp_min) {
+      if (spos < p.qs_cap) qs[spos] = v;
+      else over = true;
+      ++spos;
+    } else {
+      const uint64_t nc = chunks_of(deg[k], p.th);
+      if (nc <= kLaneChunks) {
+        for (uint64_t j = 0; j < nc; ++j) {
+          if (cpos + j < p.qc_cap) qc[cpos + j] = ((uint64_t)v << 32) | j;
+          else over = true;
+        }
+      } else if (p.hubrec[qi] != nullptr) {
+        const uint32_t h = atomicAdd(&sm.nhub, 1u);
+        if (h < p.hub_cap) p.hubrec[qi][h] = HubRec{v, (uint32_t)nc, cpos};
+        else over = true;
+      } else {  // the block writes it below
+        spare[atomicAdd(&sm.nhub, 1u)] = i0 + k;  // at most cnt <= kSoloCap entries
+        sm.pre[i0 + k]                 = (uint32_t)min(cpos, (uint64_t)0xFFFFFFFFu);
+      }
+      cpos += nc;
+    }
+  }
+  __syncthreads();
+  const uint32_t nh    = sm.nhub;
+  const bool     defer = p.hubrec[qi] != nullptr;
+  for (uint32_t h = 0; h < (defer ? 0u : nh); ++h) {
+    const uint32_t i  = spare[h];
+    const uint32_t v  = list[i];
+    const uint64_t c0 = sm.pre[i];
+    const uint64_t nc = chunks_of(__ldg(p.off + v + 1) - __ldg(p.off + v), p.th);
+    for (uint64_t j = threadIdx.x; j < nc; j += kThreads) {
+      if (c0 + j < p.qc_cap) qc[c0 + j] = ((uint64_t)v << 32) | j;
+      else over = true;
+    }
+  }
+  if (over) atomicCAS(&p.ctrl->err, 0, NWG_EOVERFLOW);
+  if (threadIdx.x == 0) {
+    c.qpos[qi] = tot;  // small entries | chunk entries << 32
+    c.qbig[qi] = (uint32_t)tb;
+    c.nhub[qi] = defer ? nh : 0u;
+  }
+  __syncthreads();
+}
+
+// Whether the step just decided (a top-down action) runs as solo levels:
+// the same answer in every block, from its copy of the decision state.
+// Only after a small top-down step: a single small level (an RMAT root
+// whose neighbours are hubs) gains less than handing the frontier back
+// to the grid costs.
+__device__ __forceinline__ bool solo_ok(const CtrlHdr& c, uint32_t next) {
+  const bool td = next == kActTD || next == kActTDSmall || next == kActTDCluster;
+  return td && !c.bu_push && c.prev_small && c.scout_exact && c.scout_count <= kSoloCap &&
+         frontier_size(c, c.cur) <= kSoloCap && (c.qpos[c.cur] >> 32) <= kSoloCap && c.nhub[c.cur] == 0;
+}
+
+// Block 0's solo levels, from the frontier in queue buffer c.cur (decided:
+// a top-down step, solo_ok).  Leaves the next decision in c (c.action) with
+// its frontier in the global queue.  All threads of block 0 call.
+__device__ __forceinline__ void solo_run(const DobfsParams& p, CtrlHdr& c, SoloSmem& sm, uint32_t* s_flag) {
+  const uint32_t cur = c.cur;
+  const uint64_t qp  = c.qpos[cur];
+  const uint32_t nS  = (uint32_t)(qp & 0xFFFFFFFFull), nC = (uint32_t)(qp >> 32);
+  if (threadIdx.x == 0) sm.cnt = nS;
+  for (uint32_t i = threadIdx.x; i < nS; i += kThreads) sm.q[0][i] = __ldcg(p.qs[cur] + i);
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < nC; i += kThreads) {  // a chunked vertex once: its chunk 0
+    const uint64_t ent = __ldcg(p.qc[cur] + i);
+    if ((ent & 0xFFFFFFFFull) == 0) {
+      const uint32_t slot = atomicAdd(&sm.cnt, 1u);
+      if (slot < kSoloCap) sm.q[0][slot] = (uint32_t)(ent >> 32);
+    }
+  }
+  __syncthreads();
+  uint32_t a  = 0;
+  uint32_t na = sm.cnt;  // == frontier_size(c, cur) <= kSoloCap
+  uint64_t E  = na <= kSoloCap ? solo_prefix(p, sm.q[0], na, sm.pre) : ~0ull;  // == c.scout_count
+  if (E > kSoloCap) {  // the queue disagrees with the counts it was decided on
+    if (threadIdx.x == 0) {
+      atomicCAS(&p.ctrl->err, 0, NWG_ESTATE);
+      c.status = NWG_ESTATE;
+      c.action = kActNone;
+    }
+    __syncthreads();
+    return;
+  }
+  for (uint32_t lv = 0;; ++lv) {
+    if (threadIdx.x == 0) sm.cnt = 0;
+    __syncthreads();
+    solo_expand(p, c.parents, sm.q[a], na, sm.pre, (uint32_t)E, sm.q[a ^ 1], &sm.cnt);
+    __syncthreads();
+    const uint32_t nq = min(sm.cnt, kSoloCap);
+    a ^= 1;
+    E = solo_prefix(p, sm.q[a], nq, sm.pre);
+    na = nq;
+    if (threadIdx.x == 0) {
+      const uint32_t nxt = c.cur ^ 1u;
+      c.qpos[nxt]        = nq;
+      c.qbig[nxt]        = 0;
+      c.nhub[nxt]        = 0;
+      c.acc_scout        = E;
+      const uint32_t next = decide_on(p, c, true, false);
+      *s_flag = (solo_ok(c, next) && lv + 1 < kSoloLevels) ? 1u : 0u;
+    }
+    __syncthreads();
+    if (!*s_flag) break;
+  }
+  // a pull reads V, not the queue (bitmap -> queue refills the buffer after it)
+  if (c.action != kActNone && c.action != kActBU) solo_publish(p, c, c.cur, sm.q[a], na, sm.q[a ^ 1], sm);
 }
 
 __global__ void __launch_bounds__(kThreads, kTravPerSm)
@@ -1440,27 +1714,61 @@ __global__ void __launch_bounds__(kThreads, kTravPerSm)
 #pragma unroll
     for (int i = 0; i < kV; ++i) dst[i] = __ldcg(src + i);
   }
-  uint32_t last = kActNone;
+  uint32_t last   = kActNone;
+  bool     resume = false;  // block 0 ran solo levels: its decision state is the next one
   for (uint32_t step = 0; ok; ++step) {
     if (threadIdx.x == 0) {
-      if (step > 0) {  // the previous step's counters, final after the barrier
-        const StepAcc* a = &p.ctrl->acc[(step - 1) % 3];
-        if (last != kActBU) {
-          const uint32_t ob = last == kActB2Q ? s_c.cur : (s_c.cur ^ 1u);  // the queue buffer it wrote
-          s_c.qpos[ob]      = __ldcg(&a->qpos);
-          s_c.qbig[ob]      = __ldcg(&a->qbig);
-          s_c.nhub[ob]      = __ldcg(&a->nhub);
+      if (resume) {
+        if (blockIdx.x != 0) {
+          const uint4* src = reinterpret_cast<const uint4*>(&p.ctrl->h);
+          uint4*       dst = reinterpret_cast<uint4*>(&s_c);
+#pragma unroll
+          for (int i = 0; i < kV; ++i) dst[i] = __ldcg(src + i);
         }
-        s_c.acc_scout = __ldcg(&a->scout);
-        s_c.acc_awake = __ldcg(&a->awake);
+        s_next = s_c.action;
+      } else {
+        if (step > 0) {  // the previous step's counters, final after the barrier
+          const StepAcc* a = &p.ctrl->acc[(step - 1) % 3];
+          if (last != kActBU) {
+            const uint32_t ob = last == kActB2Q ? s_c.cur : (s_c.cur ^ 1u);  // the queue buffer it wrote
+            s_c.qpos[ob]      = __ldcg(&a->qpos);
+            s_c.qbig[ob]      = __ldcg(&a->qbig);
+            s_c.nhub[ob]      = __ldcg(&a->nhub);
+          }
+          s_c.acc_scout = __ldcg(&a->scout);
+          s_c.acc_awake = __ldcg(&a->awake);
+        }
+        s_next = decide_on(p, s_c, blockIdx.x == 0);
       }
-      s_next = decide_on(p, s_c, blockIdx.x == 0);
     }
     __syncthreads();
     const uint32_t next = s_next;
+    if (resume && next != kActNone && s_c.nhub[s_c.cur] != 0) {  // hub records of the solo frontier
+      expand_hubs(p, s_c.cur, s_c.nhub[s_c.cur], blockIdx.x, gridDim.x);
+      ok = trav_barrier(p, gridDim.x);
+      if (!ok) break;
+      if (threadIdx.x == 0) s_c.nhub[s_c.cur] = 0;
+      __syncthreads();
+    }
+    resume = false;
     if (next == kActNone) break;
     StepAcc* a = &p.ctrl->acc[step % 3];
     if (blockIdx.x == 0 && threadIdx.x == 0) p.ctrl->acc[(step + 1) % 3] = StepAcc{};
+    if (solo_ok(s_c, next)) {  // the same in every block
+      if (blockIdx.x == 0) {
+        solo_run(p, s_c, sm.solo, &s_next);
+        if (threadIdx.x == 0) {
+          const uint4* src = reinterpret_cast<const uint4*>(&s_c);
+          uint4*       dst = reinterpret_cast<uint4*>(&p.ctrl->h);
+#pragma unroll
+          for (int i = 0; i < kV; ++i) dst[i] = src[i];
+        }
+      }
+      ok     = trav_barrier(p, gridDim.x);
+      resume = true;
+      last   = kActNone;
+      continue;
+    }
     StepView sv;
     sv.parents = s_c.parents;
     sv.bu_mode = s_c.bu_mode;
@@ -1804,6 +2112,49 @@ void ws_free(Workspace* ws) {
   delete ws;
 }
 
+// Cooperative launches of one device run one at a time, in launch order,
+// whatever their streams: each waits (on the device, through an event) for
+// the previous one to finish.  Two grids launched together on two streams
+// (two server slots, two host threads) can each become only partly
+// resident, each waiting at its grid barrier for blocks that only the
+// other's exit would make room for; their bounded waits then end in
+// NWG_ETIMEDOUT.  Other kernels may still run beside a cooperative grid:
+// they wait for nothing, so they only delay its blocks.  A stream being
+// captured into a CUDA graph launches directly (the capture cannot wait on
+// an event recorded outside it); such graphs must not overlap.
+static int coop_launch(const void* fn, dim3 grid, void** args, cudaStream_t stream) {
+  struct Chain {
+    std::mutex  mu;
+    cudaEvent_t last = nullptr;
+  };
+  static std::mutex                 map_mu;
+  static std::vector<Chain*>        chains;  // per device, never freed (process lifetime)
+  int                               dev = 0;
+  NWG_CUDA_TRY(cudaGetDevice(&dev));
+  Chain* c = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(map_mu);
+    if ((int)chains.size() <= dev) chains.resize(dev + 1, nullptr);
+    if (!chains[dev]) chains[dev] = new Chain();
+    c = chains[dev];
+  }
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  NWG_CUDA_TRY(cudaStreamIsCapturing(stream, &cap));
+  if (cap != cudaStreamCaptureStatusNone) {
+    NWG_CUDA_TRY(cudaLaunchCooperativeKernel(fn, grid, dim3(kThreads), args, 0, stream));
+    return NWG_OK;
+  }
+  std::lock_guard<std::mutex> lk(c->mu);
+  if (!c->last) {
+    NWG_CUDA_TRY(cudaEventCreateWithFlags(&c->last, cudaEventDisableTiming));
+  } else {
+    NWG_CUDA_TRY(cudaStreamWaitEvent(stream, c->last, 0));
+  }
+  NWG_CUDA_TRY(cudaLaunchCooperativeKernel(fn, grid, dim3(kThreads), args, 0, stream));
+  NWG_CUDA_TRY(cudaEventRecord(c->last, stream));
+  return NWG_OK;
+}
+
 // A traversal on `stream`: the persistent traversal kernel, one cooperative
 // launch after clearing its barrier's arrival count.
 int ws_launch(Workspace* ws, uint32_t root, int alpha, int beta, uint32_t* parents, cudaStream_t stream,
@@ -1815,7 +2166,8 @@ int ws_launch(Workspace* ws, uint32_t root, int alpha, int beta, uint32_t* paren
   uint32_t* par    = parents ? parents : ws->parents;
   void*     args[] = {&ws->params, &r, &a, &b, &par, &td};
   NWG_CUDA_TRY(cudaMemsetAsync(&ws->ctrl->bar, 0, sizeof(GridBar), stream));
-  NWG_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_trav, dim3(ws->trav_grid), dim3(kThreads), args, 0, stream));
+  const int rc = coop_launch((const void*)k_trav, dim3(ws->trav_grid), args, stream);
+  if (rc) return rc;
   ws->ran = true;
   return NWG_OK;
 }
@@ -1843,7 +2195,8 @@ int run_stepped(const DobfsParams& params, int sm_count, uint32_t root, int alph
       k_td<<<td, kThreads, 0, stream>>>(P);
     } else if (action == kActTDSmall) {
       void* args[] = {&P};
-      NWG_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_td_loop, dim3(kSmallBlocks), dim3(kThreads), args, 0, stream));
+      const int rc = coop_launch((const void*)k_td_loop, dim3(kSmallBlocks), args, stream);
+      if (rc) return rc;
     } else if (action == kActTDCluster) {
       k_td_cluster<<<kClusterCtas, kThreads, 0, stream>>>(P);  // one cluster (compiled-in cluster size)
     } else if (action == kActBU) {

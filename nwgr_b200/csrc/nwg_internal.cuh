@@ -78,7 +78,10 @@ struct alignas(16) CtrlHdr {
   unsigned long long t_start;  // %globaltimer at init (ns)
   uint32_t trace_len;
   uint32_t max_steps;
+  uint32_t scout_exact;  // scout_count is the frontier's out-degree sum (the first step, after a top-down step)
+  uint32_t prev_small;   // the last step was a top-down step whose frontier had at most kSoloCap out-edges
 };
+static_assert(sizeof(CtrlHdr) % 16 == 0, "the header is copied in 16-byte pieces");
 
 // Grid barrier of the persistent small-frontier kernel.
 struct GridBar {
@@ -187,6 +190,7 @@ struct MsWorkspace {
   void*           pass_dev  = nullptr;  // arguments and level-loop state of a pass (device)
   void*           pass_host = nullptr;  // pinned staging of the same record
   cudaGraphExec_t exec[4] = {nullptr, nullptr, nullptr, nullptr};  // pass graphs, one per word count W
+  std::vector<unsigned char> last_args[4];                          // the arguments each exec was last set to
   cudaGraph_t     tmpl[4] = {nullptr, nullptr, nullptr, nullptr};  // their templates (own the nodes below)
   cudaGraphNode_t nodes[4][10] = {};                                // kernel nodes updated per pass
   int             node_occ[4][10] = {};                             // their resident blocks per SM
@@ -316,9 +320,10 @@ uint64_t ms_ws_bytes(uint64_t n_cap, uint64_t m_cap);
 void     ms_ws_free(MsWorkspace* ws);
 int      ms_run_on(MsWorkspace* ws, GraphDev* g, const uint32_t* roots_host, uint32_t k, void* depths_dev,
                    uint32_t depth_bytes, uint8_t* deep_flags, int alpha, cudaStream_t stream, nwg_msbfs_stats* st,
-                   cudaEvent_t end_ev = nullptr);
+                   cudaEvent_t end_ev = nullptr, cudaEvent_t start_ev = nullptr);
 int      ms_run(MsWorkspace* ws, const uint32_t* roots_host, uint32_t k, void* depths_dev, uint32_t depth_bytes,
-                uint8_t* deep_flags, int alpha, cudaStream_t stream, nwg_msbfs_stats* st, cudaEvent_t end_ev = nullptr);
+                uint8_t* deep_flags, int alpha, cudaStream_t stream, nwg_msbfs_stats* st, cudaEvent_t end_ev = nullptr,
+                cudaEvent_t start_ev = nullptr);
 
 // nwg_gen.cu
 int gen_rmat(uint32_t scale, uint32_t ef, uint64_t seed, uint32_t ta, uint32_t tab, uint32_t tabc, GraphDev* g);

@@ -717,9 +717,9 @@ struct MsArgs {
 
 template <int W>
 MsArgs<W> ms_args(GraphDev* g, MsWorkspace* ws, uint8_t* depth_rows, uint32_t depth_bytes, uint32_t k) {
-  MsArgs<W>    a;
+  MsArgs<W> a;
+  std::memset(&a, 0, sizeof a);  // padding too: passes compare their arguments bytewise
   MsParams<W>& p = a.base;
-  std::memset(&p, 0, sizeof p);
   a.m        = g->m;
   p.off      = g->off;
   p.col      = g->col;
@@ -876,21 +876,34 @@ int ms_build_exec(MsWorkspace* ws, MsArgs<W>& a) {
 }
 
 // Points an instantiated pass graph at this pass's graph, depth rows and
-// source masks; rebuilds it if the driver refuses the in-place update.
+// source masks; rebuilds it if the driver refuses the in-place update.  A
+// pass with the same arguments as the previous one (same graph, source
+// count and rows) skips the ten node updates, which cost more host time
+// than a short pass takes on the device.
 template <int W>
 int ms_update_exec(MsWorkspace* ws, MsArgs<W>& a) {
-  if (!ws->exec[W - 1]) return ms_build_exec<W>(ws, a);
-  void* argv[kNNodes][1];
-  for (int slot = 0; slot < kNNodes; ++slot) {
-    cudaKernelNodeParams kp = ms_node_params<W>(ws, a, slot, argv[slot]);
-    if (cudaGraphExecKernelNodeSetParams(ws->exec[W - 1], ws->nodes[W - 1][slot], &kp) != cudaSuccess) {
-      cudaGetLastError();
-      cudaGraphExecDestroy(ws->exec[W - 1]);
-      ws->exec[W - 1] = nullptr;
-      return ms_build_exec<W>(ws, a);
+  std::vector<unsigned char>& last = ws->last_args[W - 1];
+  const unsigned char*        now  = reinterpret_cast<const unsigned char*>(&a);
+  if (ws->exec[W - 1] && last.size() == sizeof a && std::memcmp(last.data(), now, sizeof a) == 0) return NWG_OK;
+  last.clear();
+  int rc = NWG_OK;
+  if (!ws->exec[W - 1]) {
+    rc = ms_build_exec<W>(ws, a);
+  } else {
+    void* argv[kNNodes][1];
+    for (int slot = 0; slot < kNNodes; ++slot) {
+      cudaKernelNodeParams kp = ms_node_params<W>(ws, a, slot, argv[slot]);
+      if (cudaGraphExecKernelNodeSetParams(ws->exec[W - 1], ws->nodes[W - 1][slot], &kp) != cudaSuccess) {
+        cudaGetLastError();
+        cudaGraphExecDestroy(ws->exec[W - 1]);
+        ws->exec[W - 1] = nullptr;
+        rc = ms_build_exec<W>(ws, a);
+        break;
+      }
     }
   }
-  return NWG_OK;
+  if (rc == NWG_OK) last.assign(now, now + sizeof a);
+  return rc;
 }
 
 // Instantiates the pass graph of every word count up front (with arguments
@@ -944,7 +957,7 @@ int ms_run_stepped(MsWorkspace* ws, MsArgs<W>& a, cudaStream_t stream) {
 // written by the pass's last kernel (no fill beforehand).
 template <int W>
 int ms_pass_launch(GraphDev* g, MsWorkspace* ws, const uint32_t* roots_host, uint32_t k, uint8_t* depth_rows,
-                   uint32_t depth_bytes, int alpha, cudaStream_t stream) {
+                   uint32_t depth_bytes, int alpha, cudaStream_t stream, cudaEvent_t start_ev) {
   const uint64_t n  = g->n;
   MsPassDev&     h  = *static_cast<MsPassDev*>(ws->pass_host);
   MsPassDev*     dd = static_cast<MsPassDev*>(ws->pass_dev);
@@ -965,6 +978,11 @@ int ms_pass_launch(GraphDev* g, MsWorkspace* ws, const uint32_t* roots_host, uin
 
   MsArgs<W>    a     = ms_args<W>(g, ws, depth_rows, depth_bytes, k);
   const size_t words = (size_t)n * W * sizeof(uint64_t);
+  if (!ws->stepped) {  // host work first, so the device work below runs back to back
+    int rc = ms_update_exec<W>(ws, a);
+    if (rc) return rc;
+  }
+  if (start_ev) NWG_CUDA_TRY(cudaEventRecord(start_ev, stream));
   NWG_CUDA_TRY(cudaMemsetAsync(ws->vis, 0, words, stream));
   NWG_CUDA_TRY(cudaMemsetAsync(ws->fr[0], 0, words, stream));
   NWG_CUDA_TRY(cudaMemsetAsync(ws->fr[1], 0, words, stream));  // a sparse first level writes only what it touches
@@ -974,8 +992,6 @@ int ms_pass_launch(GraphDev* g, MsWorkspace* ws, const uint32_t* roots_host, uin
     int rc = ms_run_stepped<W>(ws, a, stream);
     if (rc) return rc;
   } else {
-    int rc = ms_update_exec<W>(ws, a);
-    if (rc) return rc;
     NWG_CUDA_TRY(cudaGraphLaunch(ws->exec[W - 1], stream));
   }
   NWG_CUDA_TRY(cudaMemcpyAsync(&h, dd, sizeof h, cudaMemcpyDeviceToHost, stream));
@@ -1093,11 +1109,11 @@ void ms_ws_free(MsWorkspace* ws) {
 namespace {
 
 int ms_launch_any(GraphDev* g, MsWorkspace* ws, const uint32_t* roots, uint32_t kk, uint8_t* rows,
-                  uint32_t depth_bytes, int alpha, cudaStream_t s) {
-  if (kk <= 64) return ms_pass_launch<1>(g, ws, roots, kk, rows, depth_bytes, alpha, s);
-  if (kk <= 128) return ms_pass_launch<2>(g, ws, roots, kk, rows, depth_bytes, alpha, s);
-  if (kk <= 192) return ms_pass_launch<3>(g, ws, roots, kk, rows, depth_bytes, alpha, s);
-  return ms_pass_launch<4>(g, ws, roots, kk, rows, depth_bytes, alpha, s);
+                  uint32_t depth_bytes, int alpha, cudaStream_t s, cudaEvent_t start_ev) {
+  if (kk <= 64) return ms_pass_launch<1>(g, ws, roots, kk, rows, depth_bytes, alpha, s, start_ev);
+  if (kk <= 128) return ms_pass_launch<2>(g, ws, roots, kk, rows, depth_bytes, alpha, s, start_ev);
+  if (kk <= 192) return ms_pass_launch<3>(g, ws, roots, kk, rows, depth_bytes, alpha, s, start_ev);
+  return ms_pass_launch<4>(g, ws, roots, kk, rows, depth_bytes, alpha, s, start_ev);
 }
 
 constexpr uint32_t kMsLanes = 4;  // passes of one call in flight at once
@@ -1121,12 +1137,14 @@ constexpr uint32_t kMsLanes = 4;  // passes of one call in flight at once
 // sources are rare: a graph whose diameter passes 254); with uint8 rows it
 // keeps the depths up to 254 and 255 beyond.
 //
-// end_ev (may be null) is recorded on the stream once the call's device
-// work is enqueued, before the host waits for the last passes' records, so
-// that it marks the end of the device work rather than the host's wake-up.
+// start_ev and end_ev (either may be null) bracket the call's device work:
+// start_ev is recorded on the stream after the first pass's host
+// preparation, just before its first device operation, and end_ev once the
+// device work is enqueued, before the host waits for the last passes'
+// records (so it marks the end of the device work, not the host's wake-up).
 int ms_run_on(MsWorkspace* ws, GraphDev* g, const uint32_t* roots_host, uint32_t k, void* depths_dev,
               uint32_t depth_bytes, uint8_t* deep_flags, int alpha, cudaStream_t stream, nwg_msbfs_stats* st,
-              cudaEvent_t end_ev) {
+              cudaEvent_t end_ev, cudaEvent_t start_ev) {
   if (g->n > ws->n_cap || g->m > ws->m_cap)
     return set_error(NWG_EINVAL, "graph larger than the multi-source workspace's capacity");
   for (uint32_t i = 0; i < k; ++i)
@@ -1189,7 +1207,8 @@ int ms_run_on(MsWorkspace* ws, GraphDev* g, const uint32_t* roots_host, uint32_t
     if (p >= nlanes && (rc = finish(done++)) != NWG_OK) break;
     const uint32_t l  = p % nlanes;
     const uint32_t kk = std::min<uint32_t>(256, k - 256 * p);
-    rc = ms_launch_any(g, lane_ws(l), roots_host + 256 * p, kk, rows_of(p), depth_bytes, alpha, lane_stream(l));
+    rc = ms_launch_any(g, lane_ws(l), roots_host + 256 * p, kk, rows_of(p), depth_bytes, alpha, lane_stream(l),
+                       p == 0 ? start_ev : nullptr);
   }
   auto join = [&]() {  // `s` continues after every lane's work
     for (uint32_t l = 1; l < nlanes; ++l) {
@@ -1211,8 +1230,10 @@ int ms_run_on(MsWorkspace* ws, GraphDev* g, const uint32_t* roots_host, uint32_t
 }
 
 int ms_run(MsWorkspace* ws, const uint32_t* roots_host, uint32_t k, void* depths_dev, uint32_t depth_bytes,
-           uint8_t* deep_flags, int alpha, cudaStream_t stream, nwg_msbfs_stats* st, cudaEvent_t end_ev) {
-  return ms_run_on(ws, ws->g, roots_host, k, depths_dev, depth_bytes, deep_flags, alpha, stream, st, end_ev);
+           uint8_t* deep_flags, int alpha, cudaStream_t stream, nwg_msbfs_stats* st, cudaEvent_t end_ev,
+           cudaEvent_t start_ev) {
+  return ms_run_on(ws, ws->g, roots_host, k, depths_dev, depth_bytes, deep_flags, alpha, stream, st, end_ev,
+                   start_ev);
 }
 
 }  // namespace nwg
