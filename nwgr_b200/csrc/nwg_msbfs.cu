@@ -165,21 +165,31 @@ __device__ __forceinline__ void ms_words(const uint64_t* __restrict__ src, uint6
 // multiply never carries.
 __device__ __forceinline__ uint32_t spread4(uint32_t x) { return (x * 0x00204081u) & 0x01010101u; }
 
-// Depth rows of one warp tile: 64 consecutive vertices (2 per lane) of one
-// source word, P planes.  Per group of 4 sources a lane forms, for each of
-// its vertices, the 4 depth bytes (255 where VIS lacks the bit), then pairs
-// them with byte permutes so that each 16-bit store writes one source row's
-// bytes for the lane's 2 vertices: 64 contiguous bytes of a row per warp
-// store.  Two vertices per lane keep the kernel near 64 registers, so four
-// blocks fit an SM and hide the load latency.  The planes read are cleared.
+// Depth rows, one block tile at a time: kDtTile consecutive vertices of one
+// source word (64 sources).  Each thread takes kDtVerts consecutive vertices,
+// forms their depth bytes for 4 sources at a time (255 where VIS lacks the
+// bit), transposes them with byte permutes and stores, per source, its
+// vertices' bytes into a shared-memory row.  The
+// block then writes every row of the tile as kDtTile contiguous bytes
+// (16-byte stores; widened to uint16 for 2-byte rows).  Writing 64-byte
+// pieces of 64 rows 4 MB apart from each warp reached half the HBM
+// bandwidth (165 us for 476 MB at 64 sources on RMAT-22); with 512-byte
+// runs per row a 64-source pass took 5% less in all.  The planes read are
+// cleared.
+constexpr int      kDtVerts = 2;                      // 2 or 4 (4: 1 KB runs, 64 KB, 3 blocks per SM, 5% slower)
+constexpr uint32_t kDtTile  = kMsThreads * kDtVerts;  // 512 vertices
+constexpr uint32_t kDtRowW  = kDtTile / 4;            // 32-bit words per shared row
+constexpr size_t   kDtSmem  = 64 * (size_t)kDtTile;   // 32 KB: a byte per (source, vertex)
+
 template <int W, int P>
-__device__ __forceinline__ void depth_tile(const MsParams<W>& p, int planes, uint64_t v0, int w, int nsrc,
-                                           bool aligned) {
-  const uint64_t n = p.n;
-  uint64_t       vis[2], pl[2][P];
+__device__ __forceinline__ void depth_rows_tile(const MsParams<W>& p, uint32_t* rows, int planes, uint64_t v0, int w,
+                                                int nsrc) {
+  const uint64_t n  = p.n;
+  const uint64_t vb = v0 + (uint64_t)threadIdx.x * kDtVerts;
+  uint64_t       vis[kDtVerts], pl[kDtVerts][P];
 #pragma unroll
-  for (int i = 0; i < 2; ++i) {
-    const uint64_t v  = v0 + i;
+  for (int i = 0; i < kDtVerts; ++i) {
+    const uint64_t v  = vb + i;
     const bool     ok = v < n;
     vis[i]            = ok ? p.vis[v * W + w] : 0ull;
 #pragma unroll
@@ -192,70 +202,119 @@ __device__ __forceinline__ void depth_tile(const MsParams<W>& p, int planes, uin
       }
     }
   }
+  for (int s0 = 0; s0 < nsrc; s0 += 4) {
+    uint32_t b[kDtVerts];  // byte t: depth of vertex vb + i from source 64 w + s0 + t
 #pragma unroll
-  for (int s0 = 0; s0 < 64; s0 += 4) {
-    if (s0 >= nsrc) break;
-    uint32_t b[2];
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < kDtVerts; ++i) {
       uint32_t d = 0;
 #pragma unroll
       for (int j = 0; j < P; ++j) d |= spread4((uint32_t)(pl[i][j] >> s0) & 15u) << j;
       const uint32_t m = spread4((uint32_t)(vis[i] >> s0) & 15u) * 0xFFu;
       b[i]             = d | ~m;
     }
-#pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      if (s0 + t >= nsrc) break;
-      const uint32_t row = __byte_perm(b[0], b[1], (uint32_t)(t | ((4 + t) << 4)));  // byte t of each vertex
-      const uint64_t at  = (uint64_t)(64 * w + s0 + t) * n + v0;
-      if (p.depth_bytes == 2) {  // widen: 255 (unreached) -> 0xFFFF, any other depth d -> d
-        const uint32_t ff  = __vcmpeq4(row, 0xFFFFFFFFu);  // 0xFF in each byte that is 255
-        const uint32_t two = __byte_perm(row, ff, 0x5140);  // vertex v0 in the low half, v0 + 1 in the high half
-        uint16_t*      dst = reinterpret_cast<uint16_t*>(p.depth) + at;
-        if (aligned && v0 + 1 < n) {
-          *reinterpret_cast<uint32_t*>(dst) = two;
-        } else {
-          dst[0] = (uint16_t)two;
-          if (v0 + 1 < n) dst[1] = (uint16_t)(two >> 16);
-        }
-      } else {
-        uint8_t* dst = p.depth + at;
-        if (aligned && v0 + 1 < n) {
-          *reinterpret_cast<uint16_t*>(dst) = (uint16_t)row;
-        } else {
-          dst[0] = (uint8_t)row;
-          if (v0 + 1 < n) dst[1] = (uint8_t)(row >> 8);
-        }
-      }
+    if constexpr (kDtVerts == 4) {  // 4 x 4 byte transpose: row s0 + t, byte i = b[i] byte t
+      const uint32_t lo01 = __byte_perm(b[0], b[1], 0x5140), lo23 = __byte_perm(b[2], b[3], 0x5140);
+      const uint32_t hi01 = __byte_perm(b[0], b[1], 0x7362), hi23 = __byte_perm(b[2], b[3], 0x7362);
+      uint32_t* const r = rows + (uint32_t)s0 * kDtRowW + threadIdx.x;
+      r[0]              = __byte_perm(lo01, lo23, 0x5410);
+      r[kDtRowW]        = __byte_perm(lo01, lo23, 0x7632);
+      r[2 * kDtRowW]    = __byte_perm(hi01, hi23, 0x5410);
+      r[3 * kDtRowW]    = __byte_perm(hi01, hi23, 0x7632);
+    } else {  // 4 x 2: row s0 + t holds the 2 bytes b[0] byte t, b[1] byte t
+      const uint32_t lo = __byte_perm(b[0], b[1], 0x5140), hi = __byte_perm(b[0], b[1], 0x7362);
+      uint16_t* const r = reinterpret_cast<uint16_t*>(rows) + (uint32_t)s0 * (2 * kDtRowW) + threadIdx.x;
+      r[0]              = (uint16_t)lo;
+      r[2 * kDtRowW]    = (uint16_t)(lo >> 16);
+      r[4 * kDtRowW]    = (uint16_t)hi;
+      r[6 * kDtRowW]    = (uint16_t)(hi >> 16);
     }
   }
+}
+
+// 255 (unreached) -> 0xFFFF, any other depth d -> d, for the 4 bytes of x:
+// vertices 0, 1 in the first word, 2, 3 in the second.
+__device__ __forceinline__ uint2 widen4(uint32_t x) {
+  const uint32_t ff = __vcmpeq4(x, 0xFFFFFFFFu);
+  return make_uint2(__byte_perm(x, ff, 0x5140), __byte_perm(x, ff, 0x7362));
 }
 
 // After the last level: every depth row of the pass from VIS and the level
 // planes (the planes in use are those of the highest level run), and those
 // planes cleared for the next pass.  Replaces a 255-fill of the rows and
-// the per-level byte stores of each discovery.
+// the per-level byte stores of each discovery.  Dynamic shared memory:
+// kDtSmem bytes.
 template <int W>
-__global__ void __launch_bounds__(kMsThreads, 4) k_ms_depths(MsParams<W> p) {
+__global__ void __launch_bounds__(kMsThreads, 5) k_ms_depths(MsParams<W> p) {
+  extern __shared__ uint32_t rows[];  // [64][kDtRowW]
   const uint32_t top    = p.d->level;
   const int      planes = top ? 32 - __clz(top) : 0;
   const int      k      = (int)p.d->k;
-  const unsigned lane   = threadIdx.x & 31;
-  const uint64_t tiles  = (p.n + 63) / 64 * W;
-  const uint64_t gwarp  = (uint64_t)blockIdx.x * kMsWarps + (threadIdx.x >> 5);
-  const uint64_t nwarps = (uint64_t)gridDim.x * kMsWarps;
-  // pairs of vertices are stored together when the rows keep them aligned
-  const bool     aligned = ((reinterpret_cast<uintptr_t>(p.depth) & (2u * p.depth_bytes - 1u)) | (p.n & 1u)) == 0;
-  for (uint64_t t = gwarp; t < tiles; t += nwarps) {
-    const int      w    = (int)(t % W);  // words of the same vertices in adjacent warps: shared VIS sectors
-    const uint64_t v0   = (t / W) * 64 + lane * 2;
+  const uint64_t n      = p.n;
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint64_t tiles  = (n + kDtTile - 1) / kDtTile * W;
+  const bool     two    = p.depth_bytes == 2;
+  // 16-byte stores when every row start stays 16-byte aligned
+  const bool vec = (reinterpret_cast<uintptr_t>(p.depth) & 15u) == 0 && (n & (two ? 7u : 15u)) == 0;
+  for (uint64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+    const int      w    = (int)(t % W);  // words of the same vertices in adjacent blocks: shared VIS sectors
+    const uint64_t v0   = (t / W) * kDtTile;
     const int      nsrc = min(64, k - 64 * w);
-    if (v0 >= p.n) continue;
-    if (planes <= 3) depth_tile<W, 3>(p, planes, v0, w, nsrc, aligned);
-    else if (planes <= 4) depth_tile<W, 4>(p, planes, v0, w, nsrc, aligned);
-    else depth_tile<W, 8>(p, planes, v0, w, nsrc, aligned);
+    const uint32_t nv   = (uint32_t)min((uint64_t)kDtTile, n - v0);
+    if (planes <= 3) depth_rows_tile<W, 3>(p, rows, planes, v0, w, nsrc);
+    else if (planes <= 4) depth_rows_tile<W, 4>(p, rows, planes, v0, w, nsrc);
+    else depth_rows_tile<W, 8>(p, rows, planes, v0, w, nsrc);
+    __syncthreads();
+    for (int s = (int)warp; s < nsrc; s += kMsWarps) {
+      const uint4*   src = reinterpret_cast<const uint4*>(rows + (uint32_t)s * kDtRowW);  // 16 vertices per uint4
+      const uint64_t row = (uint64_t)(64 * w + s) * n + v0;
+      if (two) {
+        uint16_t* dst = reinterpret_cast<uint16_t*>(p.depth) + row;
+        for (uint32_t c = lane; c * 16 < nv; c += 32) {  // 16 vertices: two 16-byte stores
+          const uint4 x = src[c];
+          const uint2 a = widen4(x.x), b = widen4(x.y), e = widen4(x.z), f = widen4(x.w);
+          if (vec && c * 16 + 16 <= nv) {
+            reinterpret_cast<uint4*>(dst + c * 16)[0] = make_uint4(a.x, a.y, b.x, b.y);
+            reinterpret_cast<uint4*>(dst + c * 16)[1] = make_uint4(e.x, e.y, f.x, f.y);
+          } else {
+            const uint32_t wd[8] = {a.x, a.y, b.x, b.y, e.x, e.y, f.x, f.y};
+            for (uint32_t i = 0; i < 16 && c * 16 + i < nv; ++i)
+              dst[c * 16 + i] = (uint16_t)(wd[i >> 1] >> (16 * (i & 1)));
+          }
+        }
+      } else {
+        uint8_t* dst = p.depth + row;
+        for (uint32_t c = lane; c * 16 < nv; c += 32) {
+          const uint4 x = src[c];
+          if (vec && c * 16 + 16 <= nv) {
+            *reinterpret_cast<uint4*>(dst + c * 16) = x;
+          } else {
+            const uint32_t wd[4] = {x.x, x.y, x.z, x.w};
+            for (uint32_t i = 0; i < 16 && c * 16 + i < nv; ++i) dst[c * 16 + i] = (uint8_t)(wd[i >> 2] >> (8 * (i & 3)));
+          }
+        }
+      }
+    }
+    __syncthreads();
   }
+}
+
+// The depth kernel's shared memory is above the 48 KB default: raised once
+// per word count and device, before the first launch or graph node that
+// uses it.
+template <int W>
+int ms_depths_prepare() {
+  static std::mutex        mu;
+  static std::vector<char> done;  // per device
+  int                      dev = 0;
+  NWG_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  if ((int)done.size() <= dev) done.resize(dev + 1, 0);
+  if (!done[dev]) {
+    NWG_CUDA_TRY(cudaFuncSetAttribute((const void*)k_ms_depths<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kDtSmem));
+    done[dev] = 1;
+  }
+  return NWG_OK;
 }
 
 // Roots: VIS and FR[cur] for each source (depth 0: no plane bits); the
@@ -704,6 +763,19 @@ int grid_ms(const MsWorkspace* ws, const void* kernel, uint64_t items, uint64_t 
   return grid_for(ws, ms_occupancy(kernel), items, per_block);
 }
 
+template <int W>
+int ms_depths_occupancy() {
+  int per_sm = 0;
+  if (ms_depths_prepare<W>() != NWG_OK ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k_ms_depths<W>, kMsThreads, kDtSmem) !=
+          cudaSuccess ||
+      per_sm < 1) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  return per_sm;
+}
+
 // Node slots of a pass graph.
 enum { kNRoots, kNList, kNPush0, kNFin0, kNPull0, kNPush1, kNFin1, kNPull1, kNDepths0, kNDepths1, kNNodes };
 
@@ -792,12 +864,14 @@ cudaKernelNodeParams ms_node_params(MsWorkspace* ws, MsArgs<W>& a, int slot, voi
   else {
     // grids fit the pass's own graph (a workspace may be sized for a much
     // larger one, as a serving slot's is); occupancy is queried once
-    int& per_sm = ws->node_occ[W - 1][slot];
-    if (!per_sm) per_sm = ms_occupancy(kp.func);
+    const bool depths = slot >= kNDepths0;
+    int&       per_sm = ws->node_occ[W - 1][slot];
+    if (!per_sm) per_sm = depths ? ms_depths_occupancy<W>() : ms_occupancy(kp.func);
     const uint64_t n = a.base.n;
     kp.gridDim = dim3((slot == kNPush0 || slot == kNPush1) ? grid_for(ws, per_sm, n + a.m / kMsChunk + 1, kMsWarps)
-                      : slot >= kNDepths0                  ? grid_for(ws, per_sm, (n + 63) / 64 * W, kMsWarps)
+                      : depths                             ? grid_for(ws, per_sm, (n + kDtTile - 1) / kDtTile * W, 1)
                                                            : grid_for(ws, per_sm, n, kMsThreads));
+    if (depths) kp.sharedMemBytes = (unsigned)kDtSmem;
   }
   return kp;
 }
@@ -945,8 +1019,12 @@ int ms_run_stepped(MsWorkspace* ws, MsArgs<W>& a, cudaStream_t stream) {
     }
     NWG_CUDA_TRY(cudaGetLastError());
   }
-  k_ms_depths<W><<<grid_ms(ws, (const void*)k_ms_depths<W>, (ws->n_cap + 63) / 64 * W, kMsWarps), kMsThreads, 0,
-                   stream>>>(a.base);
+  {
+    const int rc = ms_depths_prepare<W>();
+    if (rc) return rc;
+  }
+  k_ms_depths<W><<<grid_for(ws, ms_depths_occupancy<W>(), (a.base.n + kDtTile - 1) / kDtTile * W, 1), kMsThreads,
+                   kDtSmem, stream>>>(a.base);
   NWG_CUDA_TRY(cudaGetLastError());
   return NWG_OK;
 }
