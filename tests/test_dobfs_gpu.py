@@ -203,6 +203,99 @@ def test_async_workspaces(nwg, port):
     g.release()
 
 
+def _path_star(path_n, leaves, fan):
+    """A path 0..path_n-1 whose last vertex is a hub with `leaves` leaves,
+    each leaf joined to `fan` vertices of a last layer (ids after the
+    leaves), as one symmetric CSR."""
+    u = list(range(path_n - 1))
+    v = list(range(1, path_n))
+    hub = path_n - 1
+    leaf0 = path_n
+    last0 = leaf0 + leaves
+    nlast = max(1, leaves // 4)
+    rng = np.random.default_rng(5)
+    for i in range(leaves):
+        u.append(hub)
+        v.append(leaf0 + i)
+        for t in rng.integers(0, nlast, fan):
+            u.append(leaf0 + i)
+            v.append(last0 + int(t))
+    return gg.csr_from_pairs(np.array(u, np.uint64), np.array(v, np.uint64), last0 + nlast)
+
+
+def test_solo_levels(nwg, port, reference):
+    """Small top-down levels run by one block (solo levels) and handed back to
+    the whole grid: a path of 2,000 vertices (eight turns of at most 256 solo
+    levels), and a path ending in a hub of 20,000 leaves (the solo frontier
+    handed back holds a vertex of 79 chunks, written through hub records).
+    Depths, parents, per-step directions, discoveries and frontier sizes
+    equal the oracle's; the traversal is still one launch."""
+    pn = 2000
+    u = np.arange(pn - 1, dtype=np.uint64)
+    off, cols = gg.csr_from_pairs(u, u + np.uint64(1), pn)
+    g = nwg.Graph.from_csr(off, cols)
+    for r in (0, 777, pn - 1):
+        parents, st = nwg.bfs(g, g, r, 32, 15, 18, stats=True)
+        _check(nwg, port, reference, off, cols, r, parents, st)
+    g.release()
+    off, cols = _path_star(40, 20000, 3)
+    g = nwg.Graph.from_csr(off, cols)
+    for r in (0, 20, 39, 40 + 123):
+        parents, st = nwg.bfs(g, g, r, 32, 15, 18, stats=True)
+        _check(nwg, port, reference, off, cols, r, parents, st)
+    g.release()
+
+
+def test_concurrent_traversals_from_threads(nwg, port):
+    """Two host threads, each with its own workspace and stream, run
+    traversals at the same time (long paths, whose solo levels keep a
+    traversal running while the other is launched, and RMAT); every
+    result is exact.  Cooperative launches of a device are chained, so the
+    two grids never each hold part of the GPU waiting for the other."""
+    import threading
+
+    import torch
+
+    pn = 3000
+    u = np.arange(pn - 1, dtype=np.uint64)
+    hosts = [gg.csr_from_pairs(u, u + np.uint64(1), pn), gg.rmat(14, 16, seed=4)]
+    graphs = [nwg.Graph.from_csr(*h) for h in hosts]
+    want = {}
+    jobs = []
+    for gi, (off, cols) in enumerate(hosts):
+        roots = [0, pn // 2] if gi == 0 else [int(r) for r in gg.roots(off, 2, seed=8)]
+        for r in roots:
+            want[(gi, r)] = port.depths(off, cols, r)
+            jobs.append((gi, r))
+    errors = []
+
+    def worker(order):
+        try:
+            stream = torch.cuda.Stream()
+            wss = [g.workspace() for g in graphs]
+            outs = [torch.empty(g.n, dtype=torch.int32, device="cuda") for g in graphs]
+            for _ in range(6):
+                for gi, r in order:
+                    wss[gi].bfs_async(r, outs[gi], stream.cuda_stream)
+                    stream.synchronize()
+                    p = outs[gi].cpu().numpy().view(np.uint32)
+                    if wss[gi].stats().status != 0 or not np.array_equal(nwg.depths_from_parents(p, r), want[(gi, r)]):
+                        errors.append((gi, r, wss[gi].stats().status))
+            for w in wss:
+                w.close()
+        except Exception as e:  # reported below, on the main thread
+            errors.append(repr(e))
+
+    threads = [threading.Thread(target=worker, args=(jobs,)), threading.Thread(target=worker, args=(jobs[::-1],))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    for g in graphs:
+        g.release()
+    assert not errors, errors[:5]
+
+
 def test_rmat20_device_graph(nwg, port):
     g = nwg.Graph.rmat(20, 16, seed=1)
     off, cols = g.csr()
