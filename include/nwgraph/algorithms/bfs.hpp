@@ -26,7 +26,10 @@
 // contents; modifying a graph in place between calls is detected by the
 // fingerprint in most cases, but call nw::graph::b200::release(g) after
 // mutating a graph to be certain, and before destroying it to free the
-// device copy early (the registry otherwise keeps it until exit).
+// device copy early (the registry otherwise keeps it until exit).  With the
+// environment variable NWG_DROPIN_STRICT set (to anything but "0") every
+// call uploads the graph again, so each call sees the graph's current
+// contents as the reference's does, at the cost of one CSR upload per call.
 //
 // Deviations (documented): the reference cannot fail; this header throws
 // std::runtime_error when the device reports an error (bad root, out of
@@ -35,6 +38,7 @@
 #define NW_GRAPH_BFS_HPP
 
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <iostream>
 #include <limits>
@@ -96,7 +100,7 @@ class registry {
     std::lock_guard<std::mutex> lk(mu_);
     auto it = map_.find(k);
     if (it != map_.end()) {
-      if (it->second.fp == fp) return it->second.h;
+      if (it->second.fp == fp && !strict_) return it->second.h;
       nwg_graph_release(it->second.h);  // contents changed in place: upload again
       map_.erase(it);
     }
@@ -151,8 +155,14 @@ class registry {
     return h;
   }
 
+  static bool strict_from_env() {
+    const char* v = std::getenv("NWG_DROPIN_STRICT");
+    return v != nullptr && v[0] != '\0' && std::strcmp(v, "0") != 0;
+  }
+
   std::mutex             mu_;
   std::map<key, entry>   map_;
+  const bool             strict_ = strict_from_env();  // upload on every call
 };
 
 template <class G>

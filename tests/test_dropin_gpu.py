@@ -48,3 +48,22 @@ def test_dropin_header_matches_reference(nwg, port, golden, tmp_path):
                 d = nwg.depths_from_parents(p, int(r))
                 assert np.array_equal(d, G.depths[i]), f"{G.name} root {r} {suffix}: depths differ"
                 assert port.verify(G.off, G.cols, int(r), p, G.in_off, G.in_cols)
+
+
+def test_dropin_strict_mode_sees_in_place_changes(golden, tmp_path):
+    """With NWG_DROPIN_STRICT=1 every drop-in call uploads the graph again: a
+    column changed in place at an entry the registry's sampled fingerprint
+    does not read is seen by the next call (its depths equal a serial BFS of
+    the changed graph), as the reference's bfs would see it."""
+    exe = O.build_dropin_test()
+    if exe is None or not os.path.exists(exe):
+        pytest.skip("drop-in test program not built (needs the NWGraph headers at build time)")
+    G = next(G for G in golden if G.name == "rmat11")
+    mtx = tmp_path / "rmat11.mtx"
+    _write_mtx(mtx, G.off, G.cols)
+    env = dict(os.environ, NWG_DROPIN_STRICT="1")
+    for r in G.roots[:2]:
+        res = subprocess.run([exe, "--mutate", str(mtx), str(int(r))], capture_output=True, text=True, timeout=300,
+                             env=env)
+        assert res.returncode == 0, res.stdout + res.stderr
+        assert "mutation_seen 1" in res.stdout, res.stdout
