@@ -169,7 +169,7 @@ def test_roots_are_seeded_and_have_out_edges():
 
 
 def test_rmat16_shape_matches_the_calibration():
-    # SURVEY-recorded shape of the reference pipeline at scale 16: 65,536
+    # shape of the reference's own generator pipeline at scale 16: 65,536
     # vertices, ~1.82 M directed entries, max degree ~9.7 k, ~18.7 k isolated
     off, cols = gg.rmat(16, 16, seed=1)
     deg = off[1:] - off[:-1]
