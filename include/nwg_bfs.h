@@ -115,12 +115,27 @@ int nwg_graph_info(nwg_graph g, uint64_t* n, uint64_t* m, uint64_t* in_m);
 int nwg_bfs(nwg_graph g, uint32_t root, int alpha, int beta, uint32_t* parents_host, uint32_t* parents_dev,
             nwg_bfs_stats* stats);
 
+/* nwg_bfs over k roots with each root's parents copied to host row i of
+ * parents_host (k * n entries, row i = roots[i]); replaces the per-source
+ * loop of NWGraph's BFS benchmark (bench/bfs.cpp:106-141), which calls
+ * bfs(graph, gx, source, num_bins, alpha, beta) once per source.  Two
+ * traversals are in flight: root i + 1 runs on the device while root i's
+ * parents cross to the host, so with pinned host memory a call costs about
+ * k copies of n * 4 bytes rather than k copies plus k traversals (pageable
+ * memory works but the copies then serialise with the traversals).
+ * status: NULL or k entries, each root's NWG status.  All roots are checked
+ * before anything runs (NWG_EINVAL names the first bad one); otherwise every
+ * root runs and the first failing root's status is returned.  Synchronous;
+ * calls on one graph serialise with each other and with nwg_bfs. */
+int nwg_bfs_roots(nwg_graph g, const uint32_t* roots, uint64_t k, int alpha, int beta, uint32_t* parents_host,
+                  int32_t* status);
+
 /* Workspaces for concurrent, stream-ordered traversals of one graph. */
 int nwg_ws_create(nwg_graph g, nwg_bfs_ws* out);
 int nwg_ws_destroy(nwg_bfs_ws ws);
 
 /* Stream-ordered variant of nwg_bfs: enqueues the whole traversal (one CUDA
- * graph launch, no host synchronisation) on `stream` (a cudaStream_t, NULL =
+ * cooperative kernel launch, no host synchronisation) on `stream` (a cudaStream_t, NULL =
  * legacy default stream) writing parents to the device array parents_dev.
  * At most one traversal per workspace may be in flight. */
 int nwg_bfs_async(nwg_bfs_ws ws, uint32_t root, int alpha, int beta, uint32_t* parents_dev, void* stream);

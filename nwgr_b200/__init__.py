@@ -36,7 +36,7 @@ REG_VALIDATE = 0x2
 # Every symbol include/nwg_bfs.h declares (checked by the CPU test suite).
 EXPORTED = (
     "nwg_version", "nwg_last_error", "nwg_graph_register", "nwg_graph_register_u32off", "nwg_graph_release",
-    "nwg_graph_info", "nwg_bfs", "nwg_ws_create", "nwg_ws_destroy", "nwg_bfs_async", "nwg_ws_stats",
+    "nwg_graph_info", "nwg_bfs", "nwg_bfs_roots", "nwg_ws_create", "nwg_ws_destroy", "nwg_bfs_async", "nwg_ws_stats",
     "nwg_bfs_topdown", "nwg_bfs_stepped", "nwg_component_edges", "nwg_graph_copy_csr", "nwg_gen_rmat", "nwg_gen_uniform",
     "nwg_gen_grid", "nwg_pick_roots", "nwg_bfs_noalloc", "nwg_msbfs_ws_create", "nwg_msbfs_ws_destroy",
     "nwg_msbfs", "nwg_msbfs_ex", "nwg_ragged_register", "nwg_ragged_release", "nwg_ragged_info", "nwg_ragged_bfs",
@@ -152,6 +152,7 @@ def _load():
         "nwg_graph_release": (_int, [_vp]),
         "nwg_graph_info": (_int, [_vp, C.POINTER(_u64), C.POINTER(_u64), C.POINTER(_u64)]),
         "nwg_bfs": (_int, [_vp, _u32, _int, _int, _vp, _vp, C.POINTER(Stats)]),
+        "nwg_bfs_roots": (_int, [_vp, _vp, _u64, _int, _int, _vp, _vp]),
         "nwg_ws_create": (_int, [_vp, C.POINTER(_vp)]),
         "nwg_ws_destroy": (_int, [_vp]),
         "nwg_bfs_async": (_int, [_vp, _u32, _int, _int, _vp, _vp]),
@@ -544,6 +545,24 @@ def bfs(out_graph: Graph, in_graph: Graph | None = None, root: int = 0, num_bins
     s = Stats()
     check(lib.nwg_bfs(out_graph.h, int(root), alpha, beta, _ptr(parents), None, C.byref(s) if stats else None))
     return (parents, s) if stats else parents
+
+
+def bfs_roots(g: Graph, roots, parents_out=None, alpha: int = 15, beta: int = 18, status=None):
+    """nw::graph::bfs over many roots (the per-source loop of NWGraph's BFS
+    benchmark, bench/bfs.cpp:106-141): row i of the returned (k, n) uint32
+    array holds the parents of roots[i].  Two traversals are in flight, so
+    root i + 1 traverses while root i's parents are copied; pass a pinned
+    `parents_out` (e.g. a pinned torch tensor's numpy view) for overlapped
+    copies.  `status`: optional int32 array of k entries, each root's status."""
+    r = np.ascontiguousarray(roots, dtype=np.uint32)
+    k = int(r.size)
+    parents = parents_out if parents_out is not None else np.empty((k, g.n), np.uint32)
+    if parents.size < k * g.n or not parents.flags.c_contiguous or parents.dtype.itemsize != 4:
+        raise ValueError("parents_out must be a contiguous 4-byte array of at least len(roots) * n entries")
+    if status is not None and (status.size < k or status.dtype != np.int32 or not status.flags.c_contiguous):
+        raise ValueError("status must be a contiguous int32 array of at least len(roots) entries")
+    check(lib.nwg_bfs_roots(g.h, _ptr(r), k, alpha, beta, _ptr(parents), _ptr(status) if status is not None else None))
+    return parents
 
 
 def bfs_device(g: Graph, root: int, parents_dev, alpha: int = 15, beta: int = 18, stats: bool = False):

@@ -104,6 +104,7 @@ void graph_free(GraphDev* g) {
   for (MsWorkspace* ws : g->ms_workspaces) ms_ws_free(ws);
   g->ms_workspaces.clear();
   g->default_ws = nullptr;
+  g->pipe_ws    = nullptr;
   if (g->owns_out) {
     cudaFree(g->off);
     cudaFree(g->col);
@@ -239,8 +240,9 @@ int register_impl(const OffT* out_off, const uint32_t* out_col, uint64_t n, cons
   return NWG_OK;
 }
 
-int get_default_ws(GraphDev* g, Workspace** out) {
-  if (!g->default_ws) {
+// Creates *slot on first use (a workspace kept with the graph) and returns it.
+int get_owned_ws(GraphDev* g, Workspace** slot, Workspace** out) {
+  if (!*slot) {
     auto* ws = new (std::nothrow) Workspace();
     if (!ws) return set_error(NWG_ENOMEM, "host allocation failed");
     int rc = ws_init(g, ws);
@@ -249,11 +251,13 @@ int get_default_ws(GraphDev* g, Workspace** out) {
       return rc;
     }
     g->workspaces.push_back(ws);
-    g->default_ws = ws;
+    *slot = ws;
   }
-  *out = g->default_ws;
+  *out = *slot;
   return NWG_OK;
 }
+
+int get_default_ws(GraphDev* g, Workspace** out) { return get_owned_ws(g, &g->default_ws, out); }
 
 int bfs_sync(GraphDev* g, uint32_t root, int alpha, int beta, uint32_t* parents_host, uint32_t* parents_dev,
              nwg_bfs_stats* stats, bool topdown_only) {
@@ -280,6 +284,74 @@ int bfs_sync(GraphDev* g, uint32_t root, int alpha, int beta, uint32_t* parents_
     stats->device_ms = ms;
   }
   if (c.h.status != 0) return set_error(c.h.status, "device traversal reported status " + std::to_string(c.h.status));
+  return NWG_OK;
+}
+
+// k traversals with their parents copied to host rows, two in flight: the
+// graph's default workspace and a second one take the roots in turn, each on
+// its own stream, so the device-to-host copy of root i's parents runs while
+// root i + 1 traverses (the traversals themselves run one after another:
+// cooperative launches of a device are chained).  Before a workspace takes
+// root i + 2 the host waits for its root i and reads that root's status, so
+// the parents buffer and the status mirror are never overwritten in flight.
+// All roots are checked before anything is launched.
+int bfs_roots(GraphDev* g, const uint32_t* roots, uint64_t k, int alpha, int beta, uint32_t* parents_host,
+              int32_t* status) {
+  for (uint64_t i = 0; i < k; ++i)
+    if (roots[i] >= g->n)
+      return set_error(NWG_EINVAL, "roots[" + std::to_string(i) + "] = " + std::to_string(roots[i]) + " >= n " +
+                                       std::to_string(g->n));
+  if (alpha <= 0 || beta <= 0) return set_error(NWG_EINVAL, "alpha and beta must be positive");
+  std::lock_guard<std::mutex> lk(g->mu);
+  DeviceGuard                 dg(g->device);
+  Workspace*                  w[2] = {nullptr, nullptr};
+  int                         rc   = get_default_ws(g, &w[0]);
+  if (rc) return rc;
+  rc = get_owned_ws(g, &g->pipe_ws, &w[1]);
+  if (rc) return rc;
+  const size_t row       = g->n * sizeof(uint32_t);
+  bool         busy[2]   = {false, false};
+  uint64_t     which[2]  = {0, 0};
+  int          first_bad = NWG_OK;
+  std::string  first_msg;
+  auto retire = [&](int s) -> int {  // waits for lane s's root and records its status
+    if (!busy[s]) return NWG_OK;
+    busy[s] = false;
+    NWG_CUDA_TRY(cudaStreamSynchronize(w[s]->stream));
+    const int st = w[s]->ctrl_host->h.status;
+    if (status) status[which[s]] = st;
+    if (st != 0 && first_bad == NWG_OK) {
+      first_bad = st;
+      first_msg = "root index " + std::to_string(which[s]) + ": device traversal reported status " + std::to_string(st);
+    }
+    return NWG_OK;
+  };
+  for (uint64_t i = 0; i < k; ++i) {
+    const int s = (int)(i & 1);
+    rc = retire(s);
+    if (rc == NWG_OK) rc = ws_launch(w[s], roots[i], alpha, beta, w[s]->parents, w[s]->stream, false);
+    if (rc == NWG_OK) {
+      const cudaError_t e1 =
+          cudaMemcpyAsync(parents_host + i * g->n, w[s]->parents, row, cudaMemcpyDeviceToHost, w[s]->stream);
+      const cudaError_t e2 = e1 != cudaSuccess
+                                 ? e1
+                                 : cudaMemcpyAsync(w[s]->ctrl_host, w[s]->ctrl, sizeof(CtrlHdr),
+                                                   cudaMemcpyDeviceToHost, w[s]->stream);
+      if (e2 != cudaSuccess) rc = cuda_error(e2, "cudaMemcpyAsync(parents row / status)");
+    }
+    if (rc != NWG_OK) {  // the other lane's root still completes before the error returns
+      const std::string msg = g_last_error;
+      retire(s ^ 1);
+      if (status) status[i] = rc;
+      return set_error(rc, msg);
+    }
+    busy[s]  = true;
+    which[s] = i;
+  }
+  rc = retire(k & 1);  // the older of the two in flight first
+  if (rc == NWG_OK) rc = retire((k + 1) & 1);
+  if (rc) return rc;
+  if (first_bad != NWG_OK) return set_error(first_bad, first_msg);
   return NWG_OK;
 }
 
@@ -361,6 +433,14 @@ NWG_API int nwg_bfs(nwg_graph h, uint32_t root, int alpha, int beta, uint32_t* p
   NWG_GUARD_BEGIN
   if (!h) return set_error(NWG_EINVAL, "NULL graph");
   return bfs_sync(reinterpret_cast<GraphDev*>(h), root, alpha, beta, parents_host, parents_dev, stats, false);
+  NWG_GUARD_END
+}
+
+NWG_API int nwg_bfs_roots(nwg_graph h, const uint32_t* roots, uint64_t k, int alpha, int beta, uint32_t* parents_host,
+                          int32_t* status) {
+  NWG_GUARD_BEGIN
+  if (!h || (k && (!roots || !parents_host))) return set_error(NWG_EINVAL, "NULL argument");
+  return bfs_roots(reinterpret_cast<GraphDev*>(h), roots, k, alpha, beta, parents_host, status);
   NWG_GUARD_END
 }
 

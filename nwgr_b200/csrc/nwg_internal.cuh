@@ -280,6 +280,7 @@ struct GraphDev {
   Thresholds th{64, 256, 8};
   std::mutex                mu;
   Workspace*                default_ws = nullptr;
+  Workspace*                pipe_ws    = nullptr;  // second lane of nwg_bfs_roots
   std::vector<Workspace*>   workspaces;
   std::vector<MsWorkspace*> ms_workspaces;
 };

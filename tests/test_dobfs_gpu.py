@@ -203,6 +203,36 @@ def test_async_workspaces(nwg, port):
     g.release()
 
 
+def test_many_roots_to_host_rows(nwg, port, reference):
+    """nwg_bfs_roots: row i is the traversal of roots[i] (odd and even root
+    counts, so both lanes end last; a repeated root; a pinned buffer), every
+    status is 0; a bad root is refused before anything runs; zero roots is a
+    no-op."""
+    import torch
+
+    off, cols = gg.rmat(14, 16, seed=21)
+    g = nwg.Graph.from_csr(off, cols)
+    base = gg.roots(off, 6, seed=4)
+    for roots in (base[:5], np.concatenate([base, base[:1]])):
+        status = np.full(roots.size, -7, np.int32)
+        rows = nwg.bfs_roots(g, roots, status=status)
+        assert rows.shape == (roots.size, g.n)
+        assert np.all(status == 0)
+        for i, r in enumerate(roots):
+            _check(nwg, port, reference if i == 0 else None, off, cols, int(r), rows[i], None, numpy_verifier=False)
+    pinned = torch.empty((3, g.n), dtype=torch.int32).pin_memory()
+    out = nwg.bfs_roots(g, base[:3], parents_out=pinned.numpy().view(np.uint32))
+    for i in range(3):
+        assert np.array_equal(nwg.depths_from_parents(out[i], int(base[i])), port.depths(off, cols, int(base[i])))
+    keep = out.copy()
+    with pytest.raises(nwg.NwgError) as ei:
+        nwg.bfs_roots(g, np.array([base[0], g.n], np.uint32), parents_out=out)
+    assert ei.value.code == nwg.NWG_EINVAL and "roots[1]" in str(ei.value)
+    assert np.array_equal(out, keep), "a refused call wrote rows"
+    assert nwg.bfs_roots(g, np.zeros(0, np.uint32)).shape == (0, g.n)
+    g.release()
+
+
 def _path_star(path_n, leaves, fan):
     """A path 0..path_n-1 whose last vertex is a hub with `leaves` leaves,
     each leaf joined to `fan` vertices of a last layer (ids after the
