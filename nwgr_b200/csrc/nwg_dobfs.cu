@@ -125,6 +125,7 @@ struct StepView {
   uint32_t*           nhub;     // deferred hub records appended
   unsigned long long* scout;    // out-degree sum of the vertices a top-down step discovers
   unsigned long long* awake;    // vertices a pull discovers
+  uint32_t*           mark;     // top-down step: NULL = queue the discoveries, else set their bits here
 };
 
 // ---------------------------------------------------------------------------
@@ -427,8 +428,10 @@ __device__ __forceinline__ void flush_block(const DobfsParams& p, const StepView
 // atomic, never a wrong claim), then the unvisited ones are claimed with
 // atomicOr (all issued before any result is used).  A claim's winner writes parents[v] = u (the reference's CAS
 // winner) and is buffered; scout and the next queue are updated when the
-// buffer is flushed.  All 32 lanes must call.
-template <bool kDefer>
+// buffer is flushed.  In a marking push (kMark; sv.mark) the winner instead
+// sets its bit in sv.mark and only counts itself (in `scout`, which that
+// step adds to the awake count).  All 32 lanes must call.
+template <bool kDefer, bool kMark = false>
 __device__ __forceinline__ void visit_batch(const DobfsParams& p, const StepView& sv, const uint32_t (&u)[kVisit],
                                             const uint32_t (&v)[kVisit], uint32_t valid, TdWarp& tw, uint32_t& wcnt,
                                             unsigned long long& scout, uint32_t& nbig) {
@@ -452,6 +455,17 @@ __device__ __forceinline__ void visit_batch(const DobfsParams& p, const StepView
   for (int k = 0; k < kVisit; ++k)
     if ((try_mask & (1u << k)) && !(old[k] & (1u << (v[k] & 31)))) win |= 1u << k;
   const uint32_t cnt = __popc(win);
+  if (kMark) {  // marking push: the bit is the discovery record; no degree lookup, no queue entry
+#pragma unroll
+    for (int k = 0; k < kVisit; ++k) {
+      if (win & (1u << k)) {
+        parents[v[k]] = u[k];
+        atomicOr(sv.mark + (v[k] >> 5), 1u << (v[k] & 31));
+      }
+    }
+    scout += cnt;
+    return;
+  }
   const uint32_t inc = warp_incl_scan(cnt);
   const uint32_t tot = __shfl_sync(kFullMask, inc, 31);
   if (tot == 0) return;
@@ -483,7 +497,7 @@ __device__ __forceinline__ int owner_of(const uint32_t* excl, uint32_t e) {
 // range) per lane per batch; the heads and tails (< 4 edges each) are dealt
 // out as scalar edges, kVisit per lane per batch.  A unit's range is found by
 // binary search over the prefix in shared memory.  All 32 lanes must call.
-template <bool kDefer>
+template <bool kDefer, bool kMark = false>
 __device__ __forceinline__ void gather_ranges(const DobfsParams& p, const StepView& sv, uint32_t u, uint64_t lo,
                                               uint64_t hi, TdWarp& tw, uint32_t& wcnt, unsigned long long& scout,
                                               uint32_t& nbig) {
@@ -523,7 +537,7 @@ __device__ __forceinline__ void gather_ranges(const DobfsParams& p, const StepVi
       vv[3] = x.w;
       valid = 0xFu;
     }
-    visit_batch<kDefer>(p, sv, uu, vv, valid, tw, wcnt, scout, nbig);
+    visit_batch<kDefer, kMark>(p, sv, uu, vv, valid, tw, wcnt, scout, nbig);
   }
   for (uint32_t j = 0; j < stot; j += 32 * kVisit) {
     uint32_t uu[kVisit], vv[kVisit], valid = 0;
@@ -541,7 +555,7 @@ __device__ __forceinline__ void gather_ranges(const DobfsParams& p, const StepVi
         valid |= 1u << k;
       }
     }
-    visit_batch<kDefer>(p, sv, uu, vv, valid, tw, wcnt, scout, nbig);
+    visit_batch<kDefer, kMark>(p, sv, uu, vv, valid, tw, wcnt, scout, nbig);
   }
   __syncwarp();
 }
@@ -632,6 +646,7 @@ __device__ __forceinline__ void init_step(const DobfsParams& p, uint32_t root, u
     c.trace_len = 0;
     c.scout_exact = 1;  // scout_count = the root's out-degree
     c.prev_small  = 0;
+    c.mark_ok     = 0;
     const uint64_t cap = 2 * n + 64;
     c.max_steps = cap > 0xFFFFFF00ull ? 0xFFFFFF00u : (uint32_t)cap;
   }
@@ -699,19 +714,69 @@ __device__ __forceinline__ uint32_t td_kernel_setup(CtrlHdr& c) {
 // Discoveries are estimated as the front's out-edges times the unvisited
 // share, at most the candidates, and, on graphs of average degree <= 8
 // (meshes and roads, whose fronts are bands), at most twice the front.
-__device__ __forceinline__ bool pull_as_push(const DobfsParams& p, const CtrlHdr& c, uint64_t front,
+__device__ __forceinline__ uint64_t active_vertices(const DobfsParams& p) {
+  return p.n > p.nzero ? p.n - p.nzero : 1;  // vertices with edges
+}
+__device__ __forceinline__ uint64_t avg_degree(const DobfsParams& p) {
+  return max((uint64_t)1, p.m / active_vertices(p));
+}
+__device__ __forceinline__ uint64_t pull_candidates(const DobfsParams& p, uint64_t reached) {
+  const uint64_t excl = p.nzero + reached;
+  return p.n > excl ? p.n - excl : 0;
+}
+// Estimated discoveries of a step from `front` with `front_edges` out-edges
+// when `reached` vertices are visited.
+__device__ __forceinline__ uint64_t est_wins(const DobfsParams& p, uint64_t reached, uint64_t front,
+                                             uint64_t front_edges) {
+  const uint64_t cand = pull_candidates(p, reached);
+  uint64_t wins = min(cand, (uint64_t)((double)front_edges * (double)cand / (double)active_vertices(p)));
+  if (avg_degree(p) <= 8) wins = min(wins, 2 * front);
+  return wins;
+}
+__device__ __forceinline__ bool push_cheaper(const DobfsParams& p, uint64_t reached, uint64_t front,
                                              uint64_t front_edges) {
   if (!p.symmetric || front_edges == 0) return false;
-  const uint64_t excl   = p.nzero + c.reached;
-  const uint64_t cand   = p.n > excl ? p.n - excl : 0;
-  const uint64_t active = p.n > p.nzero ? p.n - p.nzero : 1;  // vertices with edges
-  const uint64_t avgdeg = max((uint64_t)1, p.m / active);
-  uint64_t       wins   = min(cand, (uint64_t)((double)front_edges * (double)cand / (double)active));
-  if (avgdeg <= 8) wins = min(wins, 2 * front);
-  const uint64_t t      = max((uint64_t)1, min(avgdeg, p.m / front_edges));
+  const uint64_t cand   = pull_candidates(p, reached);
+  const uint64_t wins   = est_wins(p, reached, front, front_edges);
+  const uint64_t t      = max((uint64_t)1, min(avg_degree(p), p.m / front_edges));
   const uint64_t push   = 300 * front + 50 * front_edges + 500 * wins;
   const uint64_t pull   = 26 * p.n + cand * (30 * t + 30 * t * t / 16);
   return push < pull;
+}
+__device__ __forceinline__ bool pull_as_push(const DobfsParams& p, const CtrlHdr& c, uint64_t front,
+                                             uint64_t front_edges) {
+  return push_cheaper(p, c.reached, front, front_edges);
+}
+
+// A pull run as a push (pull_as_push true) whose discoveries will be the
+// front of a real pull gains nothing from a queue: the pull reads its front
+// from a bitmap.  The push then only marks its discoveries in the pull's
+// discovery bitmap (kActBUMark): no out-degree lookup and no queue entry per
+// discovery, which on a uniform graph of degree 32 is the bulk of the step
+// that discovers most of the graph.  It is chosen when the same estimates
+// say, one step ahead, that the bottom-up phase goes on (bfs.hpp:229) and
+// its next step is a pull, and the step discovers at least n / 32 vertices.
+// When the real counts decide otherwise the results stay the same: a push
+// that was wanted runs as a pull; a phase that ends gets its queue from the
+// bitmap, as after any pull (bfs.hpp:235-239).
+__device__ __forceinline__ bool mark_push(const DobfsParams& p, const CtrlHdr& c, uint64_t front,
+                                          uint64_t front_edges) {
+  if (!c.mark_ok) return false;
+  const uint64_t wins = est_wins(p, c.reached, front, front_edges);
+  if (wins < p.n / 32) return false;
+  if (!(wins >= front || wins > p.n / c.beta)) return false;
+  return !push_cheaper(p, c.reached + wins, wins, wins * avg_degree(p));
+}
+
+// Starts a marking push from the queue in c.cur; it writes C[bm ^ 1] like a
+// first pull (bm = 1: C0), and its completion is a pull's.
+__device__ __forceinline__ uint32_t mark_setup(CtrlHdr& c) {
+  c.bu_push   = 0;
+  c.acc_awake = 0;
+  c.acc_scout = 0;
+  c.bu_mode   = 0;
+  c.bm        = 1;
+  return kActBUMark;
 }
 
 // ---------------------------------------------------------------------------
@@ -752,7 +817,7 @@ __device__ uint32_t decide_on(const DobfsParams& p, CtrlHdr& c, bool writer, boo
           c.old_awake   = awake;                           // bfs.hpp:206
           c.awake_count = awake;
           if (pull_as_push(p, c, awake, c.acc_scout)) {
-            next = td_kernel_setup(c);
+            next = mark_push(p, c, awake, c.acc_scout) ? mark_setup(c) : td_kernel_setup(c);
           } else {  // a pull over V, which holds every visited vertex
             c.bu_push   = 0;
             c.acc_awake = 0;
@@ -787,7 +852,8 @@ __device__ uint32_t decide_on(const DobfsParams& p, CtrlHdr& c, bool writer, boo
       }
       break;
     }
-    case kActBU: {
+    case kActBU:
+    case kActBUMark: {  // a marking push ends like a pull: its discoveries are in C[bm ^ 1]
       const uint64_t awake = c.acc_awake;
       trace_add(p.ctrl, c, 1, c.old_awake, awake, now, writer);
       c.bu_steps++;
@@ -827,8 +893,12 @@ __device__ uint32_t decide_on(const DobfsParams& p, CtrlHdr& c, bool writer, boo
       c.awake_count = nq;                                                // bfs.hpp:199-202
       c.old_awake   = nq;
       if (pull_as_push(p, c, nq, c.scout_count)) {  // scout_count: the frontier's out-edges
-        c.bu_push = 1;
-        next      = td_kernel_setup(c);
+        if (mark_push(p, c, nq, c.scout_count)) {
+          next = mark_setup(c);
+        } else {
+          c.bu_push = 1;
+          next      = td_kernel_setup(c);
+        }
       } else {
         c.acc_awake = 0;
         c.bu_mode   = 0;
@@ -892,7 +962,7 @@ __global__ void k_decide(DobfsParams p) {
 // hubs spread over the grid), then the small-degree queue; both go through
 // gather_ranges, a group of entries per warp.  The group size of chunk
 // entries shrinks when there are few so every warp gets work.
-template <bool kDefer>
+template <bool kDefer, bool kMark = false>
 __device__ __forceinline__ void td_step(const DobfsParams& p, const StepView& sv, TdWarp* tws, uint32_t block,
                                         uint32_t nblocks) {
   const uint32_t     cur     = sv.in;
@@ -920,7 +990,7 @@ __device__ __forceinline__ void td_step(const DobfsParams& p, const StepView& sv
       lo = ob + (ent & 0xFFFFFFFFull) * p.th.chunk;
       hi = min(oe, lo + p.th.chunk);
     }
-    gather_ranges<kDefer>(p, sv, u, lo, hi, tw, wcnt, scout, nbig);
+    gather_ranges<kDefer, kMark>(p, sv, u, lo, hi, tw, wcnt, scout, nbig);
   }
 
   // small vertices per warp group: fewer when there are few, so that every
@@ -938,7 +1008,7 @@ __device__ __forceinline__ void td_step(const DobfsParams& p, const StepView& sv
       lo = p.off[u];
       hi = p.off[u + 1];
     }
-    gather_ranges<kDefer>(p, sv, u, lo, hi, tw, wcnt, scout, nbig);
+    gather_ranges<kDefer, kMark>(p, sv, u, lo, hi, tw, wcnt, scout, nbig);
   }
   flush_block<kDefer>(p, sv, tws, wcnt, scout, nbig, true);
 
@@ -946,7 +1016,7 @@ __device__ __forceinline__ void td_step(const DobfsParams& p, const StepView& sv
   __syncthreads();
   const uint32_t nb = block_sum(nbig);
   if (threadIdx.x == 0) {
-    if (tot) atomicAdd(sv.scout, tot);
+    if (tot) atomicAdd(kMark ? sv.awake : sv.scout, tot);  // a marking push counts discoveries
     if (nb) atomicAdd(sv.qbig, nb);
   }
 }
@@ -969,6 +1039,7 @@ __device__ __forceinline__ StepView td_view(const DobfsParams& p) {
   sv.nhub          = &c->nhub[sv.out];
   sv.scout         = &c->acc_scout;
   sv.awake         = &c->acc_awake;
+  sv.mark          = nullptr;
   return sv;
 }
 
@@ -986,6 +1057,7 @@ __device__ __forceinline__ StepView bu_view(const DobfsParams& p) {
   sv.nhub       = &c->nhub[sv.out];
   sv.scout      = &c->acc_scout;
   sv.awake      = &c->acc_awake;
+  sv.mark       = nullptr;
   return sv;
 }
 
@@ -1713,6 +1785,7 @@ __global__ void __launch_bounds__(kThreads, kTravPerSm)
     uint4*       dst = reinterpret_cast<uint4*>(&s_c);
 #pragma unroll
     for (int i = 0; i < kV; ++i) dst[i] = __ldcg(src + i);
+    s_c.mark_ok = 1;  // every block's copy: this kernel runs marking pushes
   }
   uint32_t last   = kActNone;
   bool     resume = false;  // block 0 ran solo levels: its decision state is the next one
@@ -1729,7 +1802,7 @@ __global__ void __launch_bounds__(kThreads, kTravPerSm)
       } else {
         if (step > 0) {  // the previous step's counters, final after the barrier
           const StepAcc* a = &p.ctrl->acc[(step - 1) % 3];
-          if (last != kActBU) {
+          if (last != kActBU && last != kActBUMark) {
             const uint32_t ob = last == kActB2Q ? s_c.cur : (s_c.cur ^ 1u);  // the queue buffer it wrote
             s_c.qpos[ob]      = __ldcg(&a->qpos);
             s_c.qbig[ob]      = __ldcg(&a->qbig);
@@ -1778,6 +1851,16 @@ __global__ void __launch_bounds__(kThreads, kTravPerSm)
     sv.nhub    = &a->nhub;
     sv.scout   = &a->scout;
     sv.awake   = &a->awake;
+    sv.mark    = nullptr;
+    if (next == kActBUMark) {
+      // the discovery bitmap is cleared by the whole grid before any claim
+      uint32_t* const cw = s_c.bm ? p.C0 : p.C1;
+      for (uint64_t w = (uint64_t)blockIdx.x * kThreads + threadIdx.x; w < p.nwords; w += (uint64_t)gridDim.x * kThreads)
+        cw[w] = 0u;
+      ok = trav_barrier(p, gridDim.x);
+      if (!ok) break;
+      sv.mark = cw;
+    }
     if (next == kActBU) {
       sv.in = sv.out = s_c.cur;
       sv.nS = sv.nC = 0;
@@ -1792,10 +1875,13 @@ __global__ void __launch_bounds__(kThreads, kTravPerSm)
       const uint64_t q = s_c.qpos[s_c.cur];
       sv.nS          = min((uint64_t)(q & 0xFFFFFFFFull), p.qs_cap);
       sv.nC          = min((uint64_t)(q >> 32), p.qc_cap);
-      td_step<true>(p, sv, sm.td.tw, blockIdx.x, gridDim.x);
+      if (sv.mark)
+        td_step<true, true>(p, sv, sm.td.tw, blockIdx.x, gridDim.x);
+      else
+        td_step<true>(p, sv, sm.td.tw, blockIdx.x, gridDim.x);
     }
     ok = trav_barrier(p, gridDim.x);
-    if (ok && next != kActBU && next != kActB2Q) {
+    if (ok && next != kActBU && next != kActB2Q && next != kActBUMark) {
       const uint32_t nh = __ldcg(&a->nhub);  // the same in every block after the barrier
       if (nh) {
         expand_hubs(p, sv.out, nh, blockIdx.x, gridDim.x);

@@ -34,7 +34,10 @@ enum Action : uint32_t {
   kActTDSmall = 3,  // top-down step on a small frontier, small grid
   kActTDCluster = 4,  // top-down step on a tiny frontier, one thread-block cluster
   kActNone    = 5,
-  kNumActions = 5
+  kNumActions = 5,
+  // a bottom-up pull run as a push whose discoveries are marked in the
+  // pull's discovery bitmap instead of queued (persistent kernel only)
+  kActBUMark  = 6
 };
 
 struct Thresholds {
@@ -80,6 +83,8 @@ struct alignas(16) CtrlHdr {
   uint32_t max_steps;
   uint32_t scout_exact;  // scout_count is the frontier's out-degree sum (the first step, after a top-down step)
   uint32_t prev_small;   // the last step was a top-down step whose frontier had at most kSoloCap out-edges
+  uint32_t mark_ok;      // kActBUMark may be chosen (set by the persistent kernel in its copies)
+  uint32_t pad_[3];
 };
 static_assert(sizeof(CtrlHdr) % 16 == 0, "the header is copied in 16-byte pieces");
 
