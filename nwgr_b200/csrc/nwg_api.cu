@@ -114,16 +114,20 @@ void graph_free(GraphDev* g) {
     cudaFree(g->in_col);
   }
   cudaFree(g->Z);
+  cudaFree(g->deg16);
   delete g;
 }
 
 // Shared tail of both registration entry points: device-side offsets are in
-// place; build the in-degree-zero bitmap and query the SM count.
+// place; build the in-degree-zero bitmap and the saturated out-degrees and
+// query the SM count.
 int finish_register(GraphDev* g) {
   cudaDeviceProp prop;
   NWG_CUDA_TRY(cudaGetDeviceProperties(&prop, g->device));
   g->sm_count = prop.multiProcessorCount;
   int rc      = build_zero_indegree(g, nullptr);
+  if (rc) return rc;
+  rc = build_deg16(g, nullptr);
   if (rc) return rc;
   NWG_CUDA_TRY(cudaDeviceSynchronize());
   return NWG_OK;

@@ -126,6 +126,7 @@ struct StepView {
   unsigned long long* scout;    // out-degree sum of the vertices a top-down step discovers
   unsigned long long* awake;    // vertices a pull discovers
   uint32_t*           mark;     // top-down step: NULL = queue the discoveries, else set their bits here
+  uint32_t            mark_deg; // marking step: also sum the discoveries' out-degrees into scout
 };
 
 // ---------------------------------------------------------------------------
@@ -360,6 +361,20 @@ union StepShared {
   SoloSmem solo;
 };
 
+// Out-degrees of the valid v[k]: the 2-byte saturated copy (a 33 MB array at
+// 2^24 vertices, which stays mostly in L2, where the offsets take 134 MB),
+// and the offsets only for saturated entries.  All loads are issued first.
+template <int K>
+__device__ __forceinline__ void out_degrees(const DobfsParams& p, const uint32_t (&v)[K], uint32_t mask,
+                                            uint64_t (&d)[K]) {
+  uint32_t d16[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) d16[k] = ((mask & (1u << k)) && p.deg16) ? (uint32_t)__ldg(p.deg16 + v[k]) : 0xFFFFu;
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+    if (mask & (1u << k)) d[k] = d16[k] != 0xFFFFu ? (uint64_t)d16[k] : p.off[v[k] + 1] - p.off[v[k]];
+}
+
 // A warp's winner buffer ran full: degree lookup and append of its entries
 // (all 32 lanes call).
 template <bool kDefer>
@@ -381,9 +396,7 @@ __device__ __forceinline__ void flush_winners(const DobfsParams& p, const StepVi
         mask |= 1u << k;
       }
     }
-#pragma unroll
-    for (int k = 0; k < kVisit; ++k)
-      if (mask & (1u << k)) d[k] = p.off[v[k] + 1] - p.off[v[k]];
+    out_degrees<kVisit>(p, v, mask, d);
 #pragma unroll
     for (int k = 0; k < kVisit; ++k) scout += d[k];
     append_warp<kVisit, kDefer>(p, sv, v, d, mask, nbig);
@@ -412,9 +425,7 @@ __device__ __forceinline__ void flush_block(const DobfsParams& p, const StepView
       mask |= 1u << w;
     }
   }
-#pragma unroll
-  for (int w = 0; w < kWarps; ++w)
-    if (mask & (1u << w)) d[w] = p.off[v[w] + 1] - p.off[v[w]];
+  out_degrees<kWarps>(p, v, mask, d);
   if (count_scout) {
 #pragma unroll
     for (int w = 0; w < kWarps; ++w) scout += d[w];
@@ -428,9 +439,10 @@ __device__ __forceinline__ void flush_block(const DobfsParams& p, const StepView
 // atomic, never a wrong claim), then the unvisited ones are claimed with
 // atomicOr (all issued before any result is used).  A claim's winner writes parents[v] = u (the reference's CAS
 // winner) and is buffered; scout and the next queue are updated when the
-// buffer is flushed.  In a marking push (kMark; sv.mark) the winner instead
-// sets its bit in sv.mark and only counts itself (in `scout`, which that
-// step adds to the awake count).  All 32 lanes must call.
+// buffer is flushed.  In a marking step (kMark; sv.mark) the winner instead
+// sets its bit in sv.mark and counts itself in `nbig`, which such a step
+// adds to the awake count; a marking top-down step (sv.mark_deg) adds its
+// out-degree to `scout` as well.  All 32 lanes must call.
 template <bool kDefer, bool kMark = false>
 __device__ __forceinline__ void visit_batch(const DobfsParams& p, const StepView& sv, const uint32_t (&u)[kVisit],
                                             const uint32_t (&v)[kVisit], uint32_t valid, TdWarp& tw, uint32_t& wcnt,
@@ -455,7 +467,7 @@ __device__ __forceinline__ void visit_batch(const DobfsParams& p, const StepView
   for (int k = 0; k < kVisit; ++k)
     if ((try_mask & (1u << k)) && !(old[k] & (1u << (v[k] & 31)))) win |= 1u << k;
   const uint32_t cnt = __popc(win);
-  if (kMark) {  // marking push: the bit is the discovery record; no degree lookup, no queue entry
+  if (kMark) {  // marking step: the bit is the discovery record; no queue entry
 #pragma unroll
     for (int k = 0; k < kVisit; ++k) {
       if (win & (1u << k)) {
@@ -463,7 +475,14 @@ __device__ __forceinline__ void visit_batch(const DobfsParams& p, const StepView
         atomicOr(sv.mark + (v[k] >> 5), 1u << (v[k] & 31));
       }
     }
-    scout += cnt;
+    nbig += cnt;  // discoveries
+    if (sv.mark_deg) {  // a marking top-down step also sums their out-degrees (bfs.hpp:286)
+      uint64_t d[kVisit];
+      out_degrees<kVisit>(p, v, win, d);
+#pragma unroll
+      for (int k = 0; k < kVisit; ++k)
+        if (win & (1u << k)) scout += d[k];
+    }
     return;
   }
   const uint32_t inc = warp_incl_scan(cnt);
@@ -647,6 +666,7 @@ __device__ __forceinline__ void init_step(const DobfsParams& p, uint32_t root, u
     c.scout_exact = 1;  // scout_count = the root's out-degree
     c.prev_small  = 0;
     c.mark_ok     = 0;
+    c.b2q_then_td = 0;
     const uint64_t cap = 2 * n + 64;
     c.max_steps = cap > 0xFFFFFF00ull ? 0xFFFFFF00u : (uint32_t)cap;
   }
@@ -768,6 +788,24 @@ __device__ __forceinline__ bool mark_push(const DobfsParams& p, const CtrlHdr& c
   return !push_cheaper(p, c.reached + wins, wins, wins * avg_degree(p));
 }
 
+// A top-down step after which the reference's rule will very likely switch
+// to a pull needs no queue either: the first pull reads its front from V.
+// Such a step (kActTDMark) marks its discoveries in C0 and sums only their
+// count and out-degrees, which the switch rule needs (bfs.hpp:186).  Chosen
+// when, by the same estimates, the step discovers at least n / 32 vertices,
+// their out-degree sum is at least twice the switch threshold, and the
+// pull after it would not run as a push.  If the real sum keeps the
+// traversal top-down, bitmap -> queue rebuilds the queue from C0 first.
+__device__ __forceinline__ bool mark_td(const DobfsParams& p, const CtrlHdr& c, uint64_t front,
+                                        uint64_t front_edges) {
+  if (!c.mark_ok || c.topdown_only) return false;
+  const uint64_t wins = est_wins(p, c.reached, front, front_edges);
+  if (wins < p.n / 32) return false;
+  const uint64_t scout = wins * avg_degree(p);
+  if (scout / 2 <= c.edges_to_check / c.alpha) return false;
+  return !push_cheaper(p, c.reached + wins, wins, scout);
+}
+
 // Starts a marking push from the queue in c.cur; it writes C[bm ^ 1] like a
 // first pull (bm = 1: C0), and its completion is a pull's.
 __device__ __forceinline__ uint32_t mark_setup(CtrlHdr& c) {
@@ -777,6 +815,14 @@ __device__ __forceinline__ uint32_t mark_setup(CtrlHdr& c) {
   c.bu_mode   = 0;
   c.bm        = 1;
   return kActBUMark;
+}
+
+// Starts a marking top-down step from the queue in c.cur (writes C0).
+__device__ __forceinline__ uint32_t mark_td_setup(CtrlHdr& c) {
+  c.acc_awake = 0;
+  c.acc_scout = 0;
+  c.bm        = 1;
+  return kActTDMark;
 }
 
 // ---------------------------------------------------------------------------
@@ -852,6 +898,37 @@ __device__ uint32_t decide_on(const DobfsParams& p, CtrlHdr& c, bool writer, boo
       }
       break;
     }
+    case kActTDMark: {  // a top-down step (bfs.hpp:242-295) whose discoveries are marked in C0
+      const uint64_t nq = c.acc_awake;
+      trace_add(p.ctrl, c, 0, frontier_size(c, c.cur), nq, now, writer);
+      c.td_steps++;
+      c.reached += nq;
+      c.scout_count = c.acc_scout;  // bfs.hpp:271
+      c.scout_exact = 1;
+      if (nq == 0) {
+        done = true;  // bfs.hpp:297-303
+        break;
+      }
+      c.levels++;
+      if (c.scout_count > c.edges_to_check / c.alpha) {  // bfs.hpp:186
+        c.awake_count = nq;                                // bfs.hpp:199-202
+        c.old_awake   = nq;
+        // a pull over V (a push would need the queue; both discover the same set)
+        c.acc_awake = 0;
+        c.bu_mode   = 0;
+        c.bm        = 1;
+        next        = kActBU;
+      } else {
+        c.edges_to_check -= c.scout_count;  // bfs.hpp:243
+        c.qpos[c.cur]     = 0;               // the queue is rebuilt from C0 into buffer cur
+        c.qbig[c.cur]     = 0;
+        c.nhub[c.cur]     = 0;
+        c.bm              = 0;
+        c.b2q_then_td     = 1;
+        next              = kActB2Q;
+      }
+      break;
+    }
     case kActBU:
     case kActBUMark: {  // a marking push ends like a pull: its discoveries are in C[bm ^ 1]
       const uint64_t awake = c.acc_awake;
@@ -878,6 +955,11 @@ __device__ uint32_t decide_on(const DobfsParams& p, CtrlHdr& c, bool writer, boo
     }
     case kActB2Q:
       c.b2q_steps++;
+      if (c.b2q_then_td) {  // the queue of a marking top-down step, whose decision was top-down
+        c.b2q_then_td = 0;
+        next          = td_kernel_setup(c);
+        break;
+      }
       c.scout_count  = 1;  // bfs.hpp:241
       queue_decision = true;
       break;
@@ -906,8 +988,9 @@ __device__ uint32_t decide_on(const DobfsParams& p, CtrlHdr& c, bool writer, boo
         next        = kActBU;
       }
     } else {
-      c.edges_to_check -= c.scout_count;  // bfs.hpp:244
+      c.edges_to_check -= c.scout_count;  // bfs.hpp:243
       next = td_kernel_setup(c);
+      if (mark_td(p, c, nq, c.scout_count)) next = mark_td_setup(c);
     }
   }
   if (!done && ++c.steps > c.max_steps) {
@@ -1010,14 +1093,19 @@ __device__ __forceinline__ void td_step(const DobfsParams& p, const StepView& sv
     }
     gather_ranges<kDefer, kMark>(p, sv, u, lo, hi, tw, wcnt, scout, nbig);
   }
-  flush_block<kDefer>(p, sv, tws, wcnt, scout, nbig, true);
+  if (!kMark) flush_block<kDefer>(p, sv, tws, wcnt, scout, nbig, true);
 
   const unsigned long long tot = block_sum(scout);
   __syncthreads();
-  const uint32_t nb = block_sum(nbig);
+  const uint32_t nb = block_sum(nbig);  // a marking step: its discoveries
   if (threadIdx.x == 0) {
-    if (tot) atomicAdd(kMark ? sv.awake : sv.scout, tot);  // a marking push counts discoveries
-    if (nb) atomicAdd(sv.qbig, nb);
+    if (tot) atomicAdd(sv.scout, tot);
+    if (nb) {
+      if (kMark)
+        atomicAdd(sv.awake, (unsigned long long)nb);
+      else
+        atomicAdd(sv.qbig, nb);
+    }
   }
 }
 
@@ -1040,6 +1128,7 @@ __device__ __forceinline__ StepView td_view(const DobfsParams& p) {
   sv.scout         = &c->acc_scout;
   sv.awake         = &c->acc_awake;
   sv.mark          = nullptr;
+  sv.mark_deg      = 0;
   return sv;
 }
 
@@ -1058,6 +1147,7 @@ __device__ __forceinline__ StepView bu_view(const DobfsParams& p) {
   sv.scout      = &c->acc_scout;
   sv.awake      = &c->acc_awake;
   sv.mark       = nullptr;
+  sv.mark_deg   = 0;
   return sv;
 }
 
@@ -1802,7 +1892,7 @@ __global__ void __launch_bounds__(kThreads, kTravPerSm)
       } else {
         if (step > 0) {  // the previous step's counters, final after the barrier
           const StepAcc* a = &p.ctrl->acc[(step - 1) % 3];
-          if (last != kActBU && last != kActBUMark) {
+          if (last != kActBU && last != kActBUMark && last != kActTDMark) {
             const uint32_t ob = last == kActB2Q ? s_c.cur : (s_c.cur ^ 1u);  // the queue buffer it wrote
             s_c.qpos[ob]      = __ldcg(&a->qpos);
             s_c.qbig[ob]      = __ldcg(&a->qbig);
@@ -1851,8 +1941,9 @@ __global__ void __launch_bounds__(kThreads, kTravPerSm)
     sv.nhub    = &a->nhub;
     sv.scout   = &a->scout;
     sv.awake   = &a->awake;
-    sv.mark    = nullptr;
-    if (next == kActBUMark) {
+    sv.mark     = nullptr;
+    sv.mark_deg = next == kActTDMark ? 1u : 0u;
+    if (next == kActBUMark || next == kActTDMark) {
       // the discovery bitmap is cleared by the whole grid before any claim
       uint32_t* const cw = s_c.bm ? p.C0 : p.C1;
       for (uint64_t w = (uint64_t)blockIdx.x * kThreads + threadIdx.x; w < p.nwords; w += (uint64_t)gridDim.x * kThreads)
@@ -1881,7 +1972,7 @@ __global__ void __launch_bounds__(kThreads, kTravPerSm)
         td_step<true>(p, sv, sm.td.tw, blockIdx.x, gridDim.x);
     }
     ok = trav_barrier(p, gridDim.x);
-    if (ok && next != kActBU && next != kActB2Q && next != kActBUMark) {
+    if (ok && next != kActBU && next != kActB2Q && next != kActBUMark && next != kActTDMark) {
       const uint32_t nh = __ldcg(&a->nhub);  // the same in every block after the barrier
       if (nh) {
         expand_hubs(p, sv.out, nh, blockIdx.x, gridDim.x);
@@ -1899,6 +1990,12 @@ __global__ void __launch_bounds__(kThreads, kTravPerSm)
 #pragma unroll
     for (int i = 0; i < kV; ++i) dst[i] = src[i];
   }
+}
+
+// Out-degrees saturated at 0xFFFF (a saturated entry means: read off).
+__global__ void k_deg16(const uint64_t* __restrict__ off, uint64_t n, uint16_t* __restrict__ deg16) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x)
+    deg16[v] = (uint16_t)min(off[v + 1] - off[v], (uint64_t)0xFFFFu);
 }
 
 // In-degree-zero bitmap; bits past n are set so they are never candidates.
@@ -2160,6 +2257,7 @@ int ws_init(GraphDev* g, Workspace* ws) {
   P.C0           = ws->V + std::max<uint32_t>(nwords, 1);
   P.C1           = ws->V + 2ull * std::max<uint32_t>(nwords, 1);
   P.Z            = g->Z;
+  P.deg16        = g->deg16;
   P.qs[0]        = ws->qbuf;
   P.qs[1]        = ws->qbuf + qs_cap;
   P.qc[0]        = ws->cbuf;
@@ -2339,6 +2437,15 @@ void fill_stats(const Ctrl& c, nwg_bfs_stats* s) {
 // Builds the in-degree-zero bitmap Z and counts the vertices without
 // in-edges (g->nzero; the bits past n are set in Z and not counted).
 // Synchronises the stream.
+int build_deg16(GraphDev* g, cudaStream_t stream) {
+  NWG_CUDA_TRY(cudaMalloc(&g->deg16, std::max<uint64_t>(g->n, 1) * sizeof(uint16_t)));
+  if (g->n) {
+    k_deg16<<<grid_for(g, 4), kThreads, 0, stream>>>(g->off, g->n, g->deg16);
+    NWG_CUDA_TRY(cudaGetLastError());
+  }
+  return NWG_OK;
+}
+
 int build_zero_indegree(GraphDev* g, cudaStream_t stream) {
   const uint32_t nwords = (uint32_t)((g->n + 31) / 32);
   NWG_CUDA_TRY(cudaMalloc(&g->Z, std::max<uint32_t>(nwords, 1) * sizeof(uint32_t)));

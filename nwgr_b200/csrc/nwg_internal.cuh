@@ -37,7 +37,10 @@ enum Action : uint32_t {
   kNumActions = 5,
   // a bottom-up pull run as a push whose discoveries are marked in the
   // pull's discovery bitmap instead of queued (persistent kernel only)
-  kActBUMark  = 6
+  kActBUMark  = 6,
+  // a top-down step whose discoveries are marked likewise, with their count
+  // and out-degree sum (persistent kernel only)
+  kActTDMark  = 7
 };
 
 struct Thresholds {
@@ -83,8 +86,9 @@ struct alignas(16) CtrlHdr {
   uint32_t max_steps;
   uint32_t scout_exact;  // scout_count is the frontier's out-degree sum (the first step, after a top-down step)
   uint32_t prev_small;   // the last step was a top-down step whose frontier had at most kSoloCap out-edges
-  uint32_t mark_ok;      // kActBUMark may be chosen (set by the persistent kernel in its copies)
-  uint32_t pad_[3];
+  uint32_t mark_ok;      // kActBUMark / kActTDMark may be chosen (set by the persistent kernel in its copies)
+  uint32_t b2q_then_td;  // the bitmap -> queue pass rebuilds the queue of a marking top-down step
+  uint32_t pad_[2];
 };
 static_assert(sizeof(CtrlHdr) % 16 == 0, "the header is copied in 16-byte pieces");
 
@@ -144,6 +148,7 @@ struct DobfsParams {
   uint32_t*       C0;      // bottom-up discovery bitmaps [nwords] x 2
   uint32_t*       C1;
   const uint32_t* Z;       // in-degree-zero bitmap [nwords] (never discoverable bottom-up)
+  const uint16_t* deg16;   // out-degrees saturated at 0xFFFF [n] (NULL: degrees come from off)
   uint32_t*       qs[2];  // small-degree vertex queues
   uint64_t*       qc[2];  // chunk queues
   uint64_t        qs_cap;
@@ -277,6 +282,7 @@ struct GraphDev {
   uint64_t* in_off = nullptr;
   uint32_t* in_col = nullptr;
   uint32_t* Z = nullptr;  // in-degree-zero bitmap
+  uint16_t* deg16 = nullptr;  // out-degrees saturated at 0xFFFF (2 bytes a vertex: mostly L2-resident)
   uint64_t  nzero = 0;    // its population (vertices without in-edges)
   bool      owns_out = false, owns_in = false, symmetric = true;
   int       sm_count = 148;
@@ -312,6 +318,7 @@ int  zero_indegree_into(const uint64_t* in_off, uint64_t n, uint32_t* Z, int sm_
 void fill_stats(const Ctrl& c, nwg_bfs_stats* s);
 int  depth_row16(Workspace* ws, uint32_t root, uint16_t* row, cudaStream_t stream);
 int  build_zero_indegree(GraphDev* g, cudaStream_t stream);
+int  build_deg16(GraphDev* g, cudaStream_t stream);
 int  component_edges(GraphDev* g, const uint32_t* parents, uint64_t* edges, uint64_t* vertices);
 int  widen_offsets(const uint32_t* src, uint64_t* dst, uint64_t count, cudaStream_t stream);
 

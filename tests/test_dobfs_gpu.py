@@ -233,6 +233,39 @@ def test_many_roots_to_host_rows(nwg, port, reference):
     g.release()
 
 
+def _fan_bipartite(k=100, t=100, n2=1 << 16, d2=16):
+    """Root 0 joined to k fan vertices, each joined to all of t targets, beside
+    an unreachable uniform component of n2 vertices of degree d2 (one
+    symmetric CSR).  From the fan the estimates predict about k * t
+    discoveries whose out-degree sum is over twice the switch threshold, but
+    the step finds only the t targets (out-degree sum k * t, under the
+    threshold), so the reference stays top-down."""
+    fan = np.arange(1, k + 1, dtype=np.uint64)
+    tgt = np.arange(k + 1, k + t + 1, dtype=np.uint64)
+    uu, vv = np.meshgrid(fan, tgt)
+    o2, c2 = gg.uniform(n2, d2, seed=3)
+    base = 1 + k + t
+    src = np.repeat(np.arange(n2, dtype=np.uint64), np.diff(o2).astype(np.int64)) + np.uint64(base)
+    u = np.concatenate([np.zeros(k, np.uint64), uu.ravel(), src])
+    v = np.concatenate([fan, vv.ravel(), c2.astype(np.uint64) + np.uint64(base)])
+    return gg.csr_from_pairs(u, v, base + n2)
+
+
+def test_marking_topdown_step_that_stays_topdown(nwg, port, reference):
+    """A top-down step predicted to hand over to a pull marks its discoveries
+    instead of queueing them; when the real out-degree sum keeps the
+    traversal top-down (bfs.hpp:186), bitmap -> queue rebuilds the queue
+    first.  Depths, parents and the per-step trace equal the oracle's."""
+    off, cols = _fan_bipartite()
+    g = nwg.Graph.from_csr(off, cols)
+    parents, st = nwg.bfs(g, g, 0, 32, 15, 18, stats=True)
+    _, tr = port.dobfs(off, cols, 0)
+    assert list(tr["dir"]) == [0, 0, 0], "the oracle trace of this graph is top-down only"
+    _check(nwg, port, reference, off, cols, 0, parents, st)
+    assert st.b2q_steps == 1, "the queue of the fan's step was not rebuilt from its bitmap"
+    g.release()
+
+
 def _path_star(path_n, leaves, fan):
     """A path 0..path_n-1 whose last vertex is a hub with `leaves` leaves,
     each leaf joined to `fan` vertices of a last layer (ids after the
