@@ -17,9 +17,12 @@ call) from CUDA events on the launching stream.  The L2 is flushed (256 MB
 write) before every traversal, outside the events.
 
 e2e: the same metric through the C ABI with host buffers: each step
-registers the graph from pinned host CSR arrays (the upload), runs the 64
-nwg_bfs calls each copying the parents back to pinned host memory, and
-releases the graph; per-root time = call time + 1/64 of the upload.
+registers the graph from pinned host CSR arrays (the upload), runs
+nwg_bfs_roots over the 64 roots (two traversals in flight, each root's
+parents copied to its own row of pinned host memory), and releases the
+graph; per-root time = step time / 64.  The first --warmup steps are
+untimed, like the device leg's.  per_call_gteps is the same with one
+synchronous nwg_bfs call per root.
 
 roofline: algorithmic bytes of a traversal B_r = 4 E_r + 8 n_r + 4 N
 (every adjacency entry of the component, one offset per reached vertex,
@@ -799,8 +802,8 @@ def main():
         rows_np = rows_h.numpy().view(np.uint32)
         roots_u = np.asarray(roots, dtype=np.uint32)
         h2d = off.nbytes + cols.nbytes
-        e2e_vals, ups, steps_s, calls = [], [], [], []
-        for step in range(1 + args.steps):
+        e2e_vals, ups, steps_s, roots_s, calls = [], [], [], [], []
+        for step in range(args.warmup + args.steps):  # the first `warmup` steps are untimed
             t0 = time.perf_counter()
             ge = nwg.Graph.from_csr(off_p.numpy().view(np.uint64), col_p.numpy().view(np.uint32))
             up = time.perf_counter() - t0
@@ -812,12 +815,13 @@ def main():
                     nwg.bfs(ge, ge, int(r), parents_out=par_h.numpy().view(np.uint32))
                     calls.append(time.perf_counter() - t1)
             ge.release()
-            if step > 0:
+            if step >= args.warmup:
                 # each root's share of the step: the upload and every traversal
                 # and parents copy of the step, divided evenly over the roots
                 e2e_vals.append(hmean((e_r / 2.0) / (total / len(roots)) / 1e9))
                 ups.append(up)
                 steps_s.append(total)
+                roots_s.append(total - up)
         for i in (0, len(roots) - 1):  # the rows are the traversals of their roots
             if int(np.count_nonzero(rows_np[i] != 0xFFFFFFFF)) != int(n_r[i]) or rows_np[i][roots_u[i]] != roots_u[i]:
                 raise RuntimeError("e2e: nwg_bfs_roots row %d is not the traversal of its root" % i)
@@ -844,6 +848,9 @@ def main():
                "upload_s_median": float(np.median(ups)), "upload_gbs": h2d / float(np.median(ups)) / 1e9,
                "h2d_copy_gbs": h2d / min(h2d_s) / 1e9, "d2h_copy_gbs": 4.0 * n / min(d2h_s) / 1e9,
                "d2h_copy_ms": 1e3 * min(d2h_s), "step_ms_median": 1e3 * float(np.median(steps_s)),
+               "steps_gteps": [round(float(x) * world, 1) for x in e2e_vals],
+               "steps_upload_ms": [round(1e3 * x, 2) for x in ups],
+               "steps_roots_ms": [round(1e3 * x, 2) for x in roots_s],
                "per_call_gteps": per_call * world, "call_ms_median": 1e3 * float(np.median(calls)),
                "note": "per step: upload CSR from pinned host memory (registration), nwg_bfs_roots over the "
                        "64 roots (two traversals in flight, each root's parents copied to its own pinned host "
