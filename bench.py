@@ -79,7 +79,7 @@ FALLBACK_HBM_GBS = 6650.0
 # (one launch of the persistent kernel k_trav) captured with ncu on a smaller
 # graph of the same kind, and that graph's directed entries; scaled to a
 # workload by its entries (profiles/k_trav_traffic_rmat22_uniform22.md).
-TRAFFIC_CAPTURES = {"rmat": (186.3e6, 128306546), "uniform": (532.7e6, 134217204)}
+TRAFFIC_CAPTURES = {"rmat": (179.8e6, 128306546), "uniform": (511.6e6, 134217204)}
 
 
 def parse():
