@@ -37,7 +37,7 @@ timed like bench/common.hpp's time_op, on a bounded sample of the roots.
 Further sections of the same JSON line (each skippable with --no-<name>):
   other        the other graphs of the single-source workload (of RMAT-24,
                uniform 2^24 with average degree 32, the 4096 x 4096 grid with
-               1% shortcuts, those not named by --graph): GTEPS over 16 roots
+               1% shortcuts, those not named by --graph): GTEPS over the same 64 roots
                timed like the main line, roofline fraction, and the
                reference's bfs on the host for one root
   verifier     device BFSVerifier time per root, and the reference's
@@ -542,7 +542,7 @@ def bench_serving(nwg, num_graphs=200, rates=SERVE_RATES, seconds=1.5, slots=16,
             "generate_s": gen_s, "rates": out}
 
 
-def bench_other_graphs(nwg, torch, main_graph, hbm, with_cpu, n_roots=16, reps=3):
+def bench_other_graphs(nwg, torch, main_graph, hbm, with_cpu, n_roots=64, reps=3):
     """The other graphs of the single-source workload (RMAT-24, uniform 2^24
     at average degree 32, the 4096 x 4096 grid with 1% shortcuts), each
     timed like the main line: device time per traversal with the L2 flushed
