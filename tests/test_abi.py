@@ -37,6 +37,11 @@ def test_version_and_error_paths_without_gpu(nwg):
     n = C.c_uint64()
     assert nwg.lib.nwg_graph_info(None, C.byref(n), None, None) == nwg.NWG_EINVAL
     assert nwg.lib.nwg_bfs(None, 0, 15, 18, None, None, None) == nwg.NWG_EINVAL
+    # many roots: a NULL graph, or roots without a host output, are refused before any device call
+    assert nwg.lib.nwg_bfs_roots(None, None, 0, 15, 18, None, None) == nwg.NWG_EINVAL
+    roots = (C.c_uint32 * 2)(0, 1)
+    assert nwg.lib.nwg_bfs_roots(C.c_void_p(1), roots, 2, 15, 18, None, None) == nwg.NWG_EINVAL
+    assert "NULL" in nwg.last_error()
     assert nwg.lib.nwg_ws_stats(None, None) == nwg.NWG_EINVAL
     assert nwg.lib.nwg_gen_rmat(0, 16, 1, 1, 2, 3, C.byref(C.c_void_p())) == nwg.NWG_EINVAL
     assert nwg.lib.nwg_gen_rmat(10, 16, 1, 5, 2, 3, C.byref(C.c_void_p())) == nwg.NWG_EINVAL
