@@ -31,6 +31,18 @@ def test_graph_specs():
         bench.graph_spec("nope")
 
 
+def test_both_arms_name_the_same_metric(monkeypatch):
+    """The reference arm and this library's arm print one metric string for
+    the same workload and root count, so their values can be divided."""
+    monkeypatch.setattr(sys, "argv", ["bench.py"])
+    args = bench.parse()
+    assert args.roots == 64 and args.graph == "rmat24" and args.warmup >= 3
+    assert bench.metric_name(args, args.roots) == "BFS GTEPS (harmonic mean over 64 roots) @ rmat24"
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--impl", "reference"])
+    ref = bench.parse()
+    assert bench.metric_name(ref, ref.roots) == bench.metric_name(args, args.roots)
+
+
 def _rank(rank, world, port, q):
     import torch.distributed as dist
 
